@@ -1,0 +1,110 @@
+/*
+ * C ABI of libpfvs_gpu.so, the B200 (sm_100a) backend of the batched
+ * coniZpM search.
+ *
+ * The first six entry points and the two structs are the interface the
+ * reference's ctypes loader binds (pfvs/gpu.py:37-82), declared as the
+ * reference's backend declares them (pfvs/fp_kernel/cuda/pfvs_gpu.cu:64-97);
+ * a build of this library can be loaded by the reference package unchanged
+ * (PFVS_GPU_LIB=/path/to/libpfvs_gpu.so).  Differences in behaviour, all
+ * within the reference's own contract:
+ *   - pstat is never 1 ("redo on the CPU"): every direction is finished on
+ *     the device, or reported with a negative status that the reference's
+ *     coniZpM turns into IncompleteSearchError (pfvs/coni.py:446-453):
+ *       -8  a coordinate range exceeds int32 (as the reference kernel)
+ *       -9  the ellipsoid matrix is not positive definite
+ *       -20 an exact setup value exceeds the device's fixed-width integers
+ *       -21 the FP64 factor could not be certified (ill-conditioned)
+ *   - pfg_max_h11() is 64.
+ *
+ * The remaining entry points are extensions of this library.
+ */
+#ifndef PFVS_GPU_H
+#define PFVS_GPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Replaces the reference's pfg_input (pfvs/fp_kernel/cuda/pfvs_gpu.cu:66-78). */
+typedef struct {
+    int            n_geo;
+    const int32_t *h;          /* (n_geo,) h11 of each geometry, 3 <= h <= pfg_max_h11() */
+    const int64_t *Q, *qmax, *linmin;   /* (n_geo,) tadpole, floor(dil Q), ceil(M0min) */
+    const int64_t *kappa;      /* the geometries' kappa (h^3 each), concatenated */
+    const int64_t *Mbasis;     /* the geometries' Mbasis (h^2 each, columns = basis), concatenated */
+    int64_t        n_p;
+    const int64_t *ps;         /* (n_p, pfg_max_h11()) row-major; p (leading 0) in the first h */
+    const int32_t *pgeo;       /* (n_p,) geometry of each p */
+    int            device;     /* CUDA device ordinal */
+    int64_t        batch;      /* p-vectors per device batch (0: all that fit) */
+    int            verbose;
+} pfg_input;
+
+/* Replaces the reference's pfg_output (pfvs/fp_kernel/cuda/pfvs_gpu.cu:80-88). */
+typedef struct {
+    int64_t  n;                /* number of lattice points */
+    int64_t *M, *Kn;           /* (n, pfg_max_h11()) row-major; first h entries valid, rest 0 */
+    int64_t *q;                /* (n,) exact q = c^T mat c */
+    int64_t *pidx;             /* (n,) index of the p-vector */
+    int8_t  *pstat;            /* (n_p,) 0 done; < 0 a status (see above) */
+    double   seconds_gpu;      /* device time of the call */
+    char     err[256];
+} pfg_output;
+
+/* pfvs_gpu.cu:91 */
+int  pfg_max_h11(void);
+/* pfvs_gpu.cu:92 -- "cuda" */
+const char *pfg_backend(void);
+/* pfvs_gpu.cu:93, :476 */
+int  pfg_device_count(void);
+/* pfvs_gpu.cu:753-758 -- free the device buffers kept between calls */
+void pfg_release(int device);
+/* pfvs_gpu.cu:489-751 -- the batched pipeline; 0 on success, else err is set */
+int  pfg_coni_batch(const pfg_input *in, pfg_output *out);
+/* pfvs_gpu.cu:483-487 -- free the arrays of a pfg_output */
+void pfg_output_free(pfg_output *out);
+
+/* ---- extensions (no counterpart in the reference's C ABI) ---- */
+
+/* Search form and pruning precision for pfg_coni_batch_ex. */
+enum {
+    PFG_FORM_BATCHED = 0,      /* persistent work-stealing kernel over all directions */
+    PFG_FORM_PLAIN = 1         /* one launch per direction, one warp, no work sharing */
+};
+enum {
+    PFG_PREC_AUTO = 0,         /* FP32 pruning where qmax < 2^22, FP64 retry on -11 */
+    PFG_PREC_FP64 = 1,         /* FP64 pruning everywhere */
+    PFG_PREC_FP32 = 2          /* as AUTO */
+};
+
+typedef struct {
+    int form;                  /* PFG_FORM_* */
+    int precision;             /* PFG_PREC_* */
+    int blocks_per_sm;         /* persistent search grid (0: default) */
+    int warps_per_block;       /* (0: default) */
+} pfg_options;
+
+/* Statistics of one call. */
+typedef struct {
+    int64_t nodes;             /* search-tree nodes entered (all passes) */
+    int64_t candidates;        /* candidate values tested */
+    int64_t leaves;            /* leaf candidates decided exactly */
+    int64_t points;            /* points emitted by the search (all passes) */
+    int64_t donated;           /* subtrees handed between warps */
+    int64_t fp64_retries;      /* directions re-searched in FP64 after -11 */
+    double  ms_setup, ms_search, ms_output;   /* device time per stage */
+} pfg_stats;
+
+/* pfg_coni_batch with options and statistics (opt, stats may be NULL);
+ * dir_nodes, if not NULL, receives (n_p,) search-tree nodes per direction. */
+int pfg_coni_batch_ex(const pfg_input *in, const pfg_options *opt, pfg_output *out,
+                      pfg_stats *stats, int64_t *dir_nodes);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -1,0 +1,444 @@
+// libpfvs_gpu.so: host side of the batched coni pipeline and its C ABI
+// (include/pfvs_gpu.h).  Per batch of directions, on one stream:
+//   k_setup      lattice setup, one warp per direction   (pfg_setup.cuh)
+//   k_search<f>  FP32-pruned persistent search            (pfg_search.cuh)
+//   k_flip       FP32 successes -> done; -11 -> FP64 retry
+//   k_search<d>  FP64-pruned search of the rest
+//   k_expand .. k_gather   canonical output               (pfg_out.cuh)
+// with one host synchronisation at the end of a batch (point count, output
+// size).  No CPU fallback: a direction the device cannot finish exactly is
+// reported with a negative status.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdarg>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <vector>
+
+#include "../../include/pfvs_gpu.h"
+#include "pfg_int.cuh"
+#include "pfg_types.cuh"
+#include "pfg_setup.cuh"
+#include "pfg_search.cuh"
+#include "pfg_out.cuh"
+
+using namespace pfg;
+
+namespace {
+
+// per-direction flip between the FP32 and FP64 passes
+__global__ void k_flip(Dir *dirs, const Geo *geo, int n, int f32_used, int32_t *dir_pass,
+                       unsigned long long *retries)
+{
+    for (int pid = blockIdx.x * blockDim.x + threadIdx.x; pid < n; pid += gridDim.x * blockDim.x) {
+        Dir &D = dirs[pid];
+        if (!(f32_used && geo[D.geo].use_f32)) continue;
+        if (D.status == ST_PENDING) D.status = ST_OK;
+        else if (D.status == ST_FLOAT) { D.status = ST_PENDING; dir_pass[pid] = 2; atomicAdd(retries, 1ull); }
+    }
+}
+
+__global__ void k_fill_i32(int32_t *a, int32_t v, int n)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) a[i] = v;
+}
+
+enum {
+    W_GEO, W_KAPPA, W_MB, W_PS, W_PGEO, W_SLABOFF, W_SLAB, W_DIRS, W_SCRATCH, W_TODO32, W_TODOALL,
+    W_CTL, W_ITEMS, W_READY, W_HDR, W_COORDS, W_DIRNODES, W_DIRPASS, W_MFULL, W_KNFULL,
+    W_DIRERR, W_COUNT, W_FILL, W_SEG, W_IDX, W_PAD, W_OM, W_OK, W_OQ, W_OP, W_RETRY, W_N
+};
+
+struct Workspace {
+    std::mutex mu;
+    void *p[W_N] = {};
+    size_t cap[W_N] = {};
+};
+
+std::mutex g_ws_mu;
+std::map<int, Workspace *> g_ws;
+
+Workspace &workspace(int dev)
+{
+    std::lock_guard<std::mutex> g(g_ws_mu);
+    Workspace *&w = g_ws[dev];
+    if (!w) w = new Workspace();
+    return *w;
+}
+
+cudaError_t ws_get(Workspace &W, int slot, size_t bytes, void **out)
+{
+    if (bytes == 0) bytes = 16;
+    if (W.cap[slot] < bytes) {
+        if (W.p[slot]) cudaFree(W.p[slot]);
+        W.p[slot] = nullptr;
+        W.cap[slot] = 0;
+        size_t b = bytes + bytes / 8 + 256;
+        cudaError_t e = cudaMalloc(&W.p[slot], b);
+        if (e != cudaSuccess) { W.p[slot] = nullptr; return e; }
+        W.cap[slot] = b;
+    }
+    *out = W.p[slot];
+    return cudaSuccess;
+}
+
+void ws_release(Workspace &W)
+{
+    for (int k = 0; k < W_N; ++k) {
+        if (W.p[k]) cudaFree(W.p[k]);
+        W.p[k] = nullptr;
+        W.cap[k] = 0;
+    }
+}
+
+void set_err(pfg_output *out, const char *fmt, ...)
+{
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(out->err, sizeof out->err, fmt, ap);
+    va_end(ap);
+}
+
+}  // namespace
+
+#define CK(x) do { cudaError_t e_ = (x); if (e_ != cudaSuccess) { \
+    set_err(out, "%s (%s:%d)", cudaGetErrorString(e_), __FILE__, __LINE__); rc = 1; goto fail; } } while (0)
+#define WS(ptr, slot, bytes) CK(ws_get(W, slot, (size_t)(bytes), (void **)&(ptr)))
+
+extern "C" int pfg_max_h11(void) { return MH; }
+extern "C" const char *pfg_backend(void) { return "cuda"; }
+
+extern "C" int pfg_device_count(void)
+{
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess) return 0;
+    return n;
+}
+
+extern "C" void pfg_output_free(pfg_output *out)
+{
+    free(out->M); free(out->Kn); free(out->q); free(out->pidx); free(out->pstat);
+    out->M = out->Kn = out->q = out->pidx = nullptr;
+    out->pstat = nullptr;
+    out->n = 0;
+}
+
+extern "C" void pfg_release(int device)
+{
+    Workspace &W = workspace(device);
+    std::lock_guard<std::mutex> g(W.mu);
+    if (cudaSetDevice(device) == cudaSuccess) ws_release(W);
+}
+
+extern "C" int pfg_coni_batch(const pfg_input *in, pfg_output *out)
+{
+    return pfg_coni_batch_ex(in, nullptr, out, nullptr, nullptr);
+}
+
+extern "C" int pfg_coni_batch_ex(const pfg_input *in, const pfg_options *opt_in, pfg_output *out,
+                                 pfg_stats *stats, int64_t *dir_nodes_out)
+{
+    memset(out, 0, sizeof *out);
+    if (stats) memset(stats, 0, sizeof *stats);
+    pfg_options opt = {PFG_FORM_BATCHED, PFG_PREC_AUTO, 0, 0};
+    if (opt_in) opt = *opt_in;
+    const int64_t NP = in->n_p;
+    if (NP < 0 || in->n_geo < 0) { set_err(out, "negative sizes"); return 1; }
+    std::vector<Geo> geos(in->n_geo);
+    {
+        int64_t koff = 0, moff = 0;
+        for (int gi = 0; gi < in->n_geo; ++gi) {
+            Geo &g = geos[gi];
+            g.h = in->h[gi];
+            g.d = g.h - 1;
+            g.Q = in->Q[gi]; g.qmax = in->qmax[gi]; g.linmin = in->linmin[gi];
+            if (g.h < 3 || g.h > MH || g.Q <= 0 || g.qmax < 0) {
+                set_err(out, "geometry %d: unsupported h11 = %d (3..%d), Q or qmax", gi, g.h, MH);
+                return 1;
+            }
+            g.use_f32 = g.qmax < (1LL << 22) && opt.precision != PFG_PREC_FP64;
+            g.koff = koff; g.moff = moff;
+            g.slab_len = slab_layout(g.h, g.d).len;
+            koff += (int64_t)g.h * g.h * g.h;
+            moff += (int64_t)g.h * g.h;
+        }
+    }
+    for (int64_t ip = 0; ip < NP; ++ip)
+        if (in->pgeo[ip] < 0 || in->pgeo[ip] >= in->n_geo) {
+            set_err(out, "p %lld: bad geometry index", (long long)ip);
+            return 1;
+        }
+    out->pstat = (int8_t *)calloc(NP > 0 ? NP : 1, 1);
+    if (!out->pstat) { set_err(out, "out of host memory"); return 1; }
+    if (NP == 0) return 0;
+
+    int rc = 0;
+    Workspace &W = workspace(in->device);
+    std::unique_lock<std::mutex> lock(W.mu);
+    std::vector<int64_t> Mo, Ko, qo, po;
+    cudaEvent_t ev[8] = {};
+    int64_t koff_total = 0, moff_total = 0;
+    Geo *dgeo = nullptr;
+    int64_t *dkappa = nullptr, *dmb = nullptr;
+    int nsm = 148;
+    for (auto &g : geos) { koff_total += (int64_t)g.h * g.h * g.h; moff_total += (int64_t)g.h * g.h; }
+
+    CK(cudaSetDevice(in->device));
+    CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, in->device));
+    for (auto &e : ev) CK(cudaEventCreate(&e));
+    WS(dgeo, W_GEO, geos.size() * sizeof(Geo));
+    WS(dkappa, W_KAPPA, koff_total * 8);
+    WS(dmb, W_MB, moff_total * 8);
+    CK(cudaMemcpy(dgeo, geos.data(), geos.size() * sizeof(Geo), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(dkappa, in->kappa, koff_total * 8, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(dmb, in->Mbasis, moff_total * 8, cudaMemcpyHostToDevice));
+    {
+        // batch size: all directions whose slabs fit in a quarter of free memory
+        size_t free_b = 0, total_b = 0;
+        CK(cudaMemGetInfo(&free_b, &total_b));
+        int64_t batch = in->batch > 0 ? in->batch : NP;
+        {
+            int64_t acc = 0, nb = 0;
+            const int64_t budget = (int64_t)(free_b / 4 / 8);
+            for (int64_t ip = 0; ip < NP && nb < batch; ++ip, ++nb) {
+                acc += geos[in->pgeo[ip]].slab_len;
+                if (acc > budget && nb > 0) break;
+            }
+            batch = std::max<int64_t>(1, std::min(batch, nb));
+        }
+        unsigned long long pts_cap = 1ull << 20;
+        const unsigned q_cap = 1u << 20;
+        for (int64_t off = 0; off < NP;) {
+            const int nb = (int)std::min<int64_t>(batch, NP - off);
+            int64_t *dps; int32_t *dpgeo; int64_t *dslaboff, *dslab; Dir *ddirs; SetupScratch *dscr;
+            int32_t *dtodo32, *dtodoall; SearchCtl *dctl; WorkItem *ditems; int *dready;
+            PointHdr *dhdr; int32_t *dcoords; unsigned long long *ddirnodes, *dretry; int32_t *ddirpass;
+            std::vector<int64_t> slab_off(nb);
+            std::vector<int32_t> todo32, todoall(nb);
+            int64_t slab_total = 0;
+            for (int k = 0; k < nb; ++k) {
+                slab_off[k] = slab_total;
+                slab_total += geos[in->pgeo[off + k]].slab_len;
+                todoall[k] = k;
+                if (geos[in->pgeo[off + k]].use_f32) todo32.push_back(k);
+            }
+            const int setup_warps = (std::min(nb, nsm * 8) + 3) / 4 * 4;   // whole blocks of 4 warps
+            WS(dps, W_PS, (size_t)nb * MH * 8);
+            WS(dpgeo, W_PGEO, (size_t)nb * 4);
+            WS(dslaboff, W_SLABOFF, (size_t)nb * 8);
+            WS(dslab, W_SLAB, (size_t)slab_total * 8);
+            WS(ddirs, W_DIRS, (size_t)nb * sizeof(Dir));
+            WS(dscr, W_SCRATCH, (size_t)setup_warps * sizeof(SetupScratch));
+            WS(dtodo32, W_TODO32, (size_t)std::max<size_t>(todo32.size(), 1) * 4);
+            WS(dtodoall, W_TODOALL, (size_t)nb * 4);
+            WS(dctl, W_CTL, 2 * sizeof(SearchCtl) + 64);
+            WS(ditems, W_ITEMS, (size_t)q_cap * sizeof(WorkItem));
+            WS(dready, W_READY, (size_t)q_cap * 4);
+            WS(ddirnodes, W_DIRNODES, (size_t)nb * 8);
+            WS(ddirpass, W_DIRPASS, (size_t)nb * 4);
+            WS(dretry, W_RETRY, 64);
+            CK(cudaMemcpy(dps, &in->ps[off * MH], (size_t)nb * MH * 8, cudaMemcpyHostToDevice));
+            CK(cudaMemcpy(dpgeo, &in->pgeo[off], (size_t)nb * 4, cudaMemcpyHostToDevice));
+            CK(cudaMemcpy(dslaboff, slab_off.data(), (size_t)nb * 8, cudaMemcpyHostToDevice));
+            if (!todo32.empty())
+                CK(cudaMemcpy(dtodo32, todo32.data(), todo32.size() * 4, cudaMemcpyHostToDevice));
+            CK(cudaMemcpy(dtodoall, todoall.data(), (size_t)nb * 4, cudaMemcpyHostToDevice));
+
+        restart_search:
+            WS(dhdr, W_HDR, pts_cap * sizeof(PointHdr));
+            WS(dcoords, W_COORDS, pts_cap * MD * 4);
+            CK(cudaMemset(dctl, 0, 2 * sizeof(SearchCtl) + 64));
+            CK(cudaMemset(ddirnodes, 0, (size_t)nb * 8));
+            CK(cudaMemset(dretry, 0, 64));
+            k_fill_i32<<<(nb + 255) / 256, 256>>>(ddirpass, 1, nb);
+            CK(cudaGetLastError());
+            // ---- setup ----
+            CK(cudaEventRecord(ev[0]));
+            {
+                SetupArgs SA{dgeo, dkappa, dmb, dps, dpgeo, dslaboff, dslab, ddirs, dscr, nb,
+                             (unsigned *)((char *)dctl + 2 * sizeof(SearchCtl))};
+                k_setup<<<setup_warps / 4, 128>>>(SA);
+                CK(cudaGetLastError());
+            }
+            CK(cudaEventRecord(ev[1]));
+            // ---- search ----
+            {
+                SearchArgs A{};
+                A.geo = dgeo; A.dirs = ddirs; A.slab = dslab; A.pass = 1; A.items = ditems;
+                A.ready = dready; A.q_cap = q_cap; A.hdr = dhdr; A.coords = dcoords; A.pts_cap = pts_cap;
+                A.dir_nodes = ddirnodes; A.eps = 1e-4; A.wait_ns = 30ll * 1000000000ll;
+                A.npts = &dctl->npts;
+                A.deadline_ns = 120ll * 1000000000ll;
+                const int wpb = opt.warps_per_block > 0 ? opt.warps_per_block : 8;
+                if (opt.form == PFG_FORM_PLAIN) {
+                    A.donate = 0; A.n_warps = 1;
+                    A.ctl = dctl;
+                    for (int k = 0; k < nb; ++k) {
+                        const bool f32 = geos[in->pgeo[off + k]].use_f32;
+                        if (f32) k_search_plain<float><<<1, 32>>>(A, k);
+                    }
+                    k_flip<<<(nb + 255) / 256, 256>>>(ddirs, dgeo, nb, 1, ddirpass, dretry);
+                    A.pass = 2;
+                    for (int k = 0; k < nb; ++k) k_search_plain<double><<<1, 32>>>(A, k);
+                    CK(cudaGetLastError());
+                } else {
+                    int bps = opt.blocks_per_sm;
+                    if (bps <= 0) {
+                        int mb32 = 0;
+                        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&mb32, k_search<float>, wpb * 32, 0));
+                        bps = std::max(1, mb32);
+                    }
+                    const int grid = nsm * bps;
+                    A.donate = 1; A.n_warps = grid * wpb;
+                    // FP32 pass over the FP32 geometries' directions
+                    if (!todo32.empty()) {
+                        A.ctl = dctl; A.todo = dtodo32; A.n_todo = (int)todo32.size(); A.pass = 1;
+                        CK(cudaMemset(dready, 0, (size_t)q_cap * 4));
+                        k_search<float><<<grid, wpb * 32>>>(A);
+                        CK(cudaGetLastError());
+                    }
+                    k_flip<<<(nb + 255) / 256, 256>>>(ddirs, dgeo, nb, 1, ddirpass, dretry);
+                    // FP64 pass over everything still pending
+                    A.ctl = dctl + 1; A.todo = dtodoall; A.n_todo = nb; A.pass = 2;
+                    CK(cudaMemset(dready, 0, (size_t)q_cap * 4));
+                    k_search<double><<<grid, wpb * 32>>>(A);
+                    CK(cudaGetLastError());
+                }
+            }
+            CK(cudaEventRecord(ev[2]));
+            SearchCtl hctl[2];
+            CK(cudaMemcpy(hctl, dctl, 2 * sizeof(SearchCtl), cudaMemcpyDeviceToHost));
+            if (hctl[0].err || hctl[1].err) {
+                set_err(out, "search: a bounded device wait ran out (status %d)", hctl[0].err ? hctl[0].err : hctl[1].err);
+                rc = 1;
+                goto fail;
+            }
+            const unsigned long long npts = hctl[0].npts;
+            if (npts > pts_cap) {
+                pts_cap = npts + npts / 4 + 1024;
+                if (in->verbose) fprintf(stderr, "pfg: point buffer -> %llu\n", pts_cap);
+                goto restart_search;
+            }
+            // ---- output ----
+            int64_t *dM, *dK; int *derr; unsigned *dcount, *dfill, *didx, *dpad; unsigned long long *dseg;
+            WS(dM, W_MFULL, std::max<unsigned long long>(npts, 1) * MH * 8);
+            WS(dK, W_KNFULL, std::max<unsigned long long>(npts, 1) * MH * 8);
+            WS(derr, W_DIRERR, (size_t)nb * 4);
+            WS(dcount, W_COUNT, (size_t)nb * 4);
+            WS(dfill, W_FILL, (size_t)nb * 4);
+            WS(dseg, W_SEG, (size_t)(nb + 1) * 8);
+            WS(didx, W_IDX, std::max<unsigned long long>(npts, 1) * 4);
+            WS(dpad, W_PAD, std::max<unsigned long long>(npts, 1) * 8 + 64);
+            CK(cudaMemset(derr, 0, (size_t)nb * 4));
+            CK(cudaMemset(dcount, 0, (size_t)nb * 4));
+            CK(cudaMemset(dfill, 0, (size_t)nb * 4));
+            CK(cudaEventRecord(ev[3]));
+            OutArgs O{ddirs, dslab, dhdr, dcoords, ddirpass, npts, nb, dM, dK, derr, dcount, dfill, dseg, didx};
+            if (npts) {
+                k_expand<<<nsm * 8, 256>>>(O);
+                k_count<<<nsm * 4, 256>>>(O);
+            }
+            k_scan<<<1, 1024>>>(O);
+            if (npts) {
+                k_scatter<<<nsm * 4, 256>>>(O);
+                k_segsort<<<std::min(nb, nsm * 8), 256>>>(O, dpad);
+            }
+            CK(cudaGetLastError());
+            unsigned long long n_out = 0;
+            CK(cudaMemcpy(&n_out, dseg + nb, 8, cudaMemcpyDeviceToHost));
+            int64_t *oM, *oK, *oq, *op;
+            WS(oM, W_OM, std::max<unsigned long long>(n_out, 1) * MH * 8);
+            WS(oK, W_OK, std::max<unsigned long long>(n_out, 1) * MH * 8);
+            WS(oq, W_OQ, std::max<unsigned long long>(n_out, 1) * 8);
+            WS(op, W_OP, std::max<unsigned long long>(n_out, 1) * 8);
+            if (n_out) {
+                GatherArgs G{didx, dhdr, dM, dK, n_out, off, oM, oK, oq, op};
+                k_gather<<<nsm * 8, 256>>>(G);
+                CK(cudaGetLastError());
+            }
+            CK(cudaEventRecord(ev[4]));
+            const size_t base = qo.size();
+            Mo.resize((base + n_out) * MH); Ko.resize((base + n_out) * MH);
+            qo.resize(base + n_out); po.resize(base + n_out);
+            if (n_out) {
+                CK(cudaMemcpy(&Mo[base * MH], oM, n_out * MH * 8, cudaMemcpyDeviceToHost));
+                CK(cudaMemcpy(&Ko[base * MH], oK, n_out * MH * 8, cudaMemcpyDeviceToHost));
+                CK(cudaMemcpy(&qo[base], oq, n_out * 8, cudaMemcpyDeviceToHost));
+                CK(cudaMemcpy(&po[base], op, n_out * 8, cudaMemcpyDeviceToHost));
+            }
+            // statuses
+            {
+                std::vector<Dir> hd(nb);
+                std::vector<int> herr(nb);
+                CK(cudaMemcpy(hd.data(), ddirs, (size_t)nb * sizeof(Dir), cudaMemcpyDeviceToHost));
+                CK(cudaMemcpy(herr.data(), derr, (size_t)nb * 4, cudaMemcpyDeviceToHost));
+                std::map<std::pair<int, int>, int> fails;
+                for (int k = 0; k < nb; ++k) {
+                    int st = hd[k].status;
+                    if (herr[k]) st = ST_OVERFLOW;
+                    out->pstat[off + k] = (st == ST_OK || st == ST_PENDING || st == ST_EMPTY) ? 0 : (int8_t)st;
+                    if (out->pstat[off + k]) fails[{st, hd[k].pad}]++;
+                }
+                if (in->verbose)
+                    for (auto &f : fails)
+                        fprintf(stderr, "pfg: %d directions with status %d (setup step %d)\n", f.second,
+                                f.first.first, f.first.second);
+                if (dir_nodes_out) {
+                    std::vector<unsigned long long> dn(nb);
+                    CK(cudaMemcpy(dn.data(), ddirnodes, (size_t)nb * 8, cudaMemcpyDeviceToHost));
+                    for (int k = 0; k < nb; ++k) dir_nodes_out[off + k] = (int64_t)dn[k];
+                }
+            }
+            {
+                float ms[4];
+                CK(cudaEventElapsedTime(&ms[0], ev[0], ev[1]));
+                CK(cudaEventElapsedTime(&ms[1], ev[1], ev[2]));
+                CK(cudaEventElapsedTime(&ms[2], ev[3], ev[4]));
+                out->seconds_gpu += (ms[0] + ms[1] + ms[2]) / 1e3;
+                unsigned long long retries = 0;
+                CK(cudaMemcpy(&retries, dretry, 8, cudaMemcpyDeviceToHost));
+                if (stats) {
+                    stats->ms_setup += ms[0]; stats->ms_search += ms[1]; stats->ms_output += ms[2];
+                    stats->nodes += (int64_t)(hctl[0].nodes + hctl[1].nodes);
+                    stats->candidates += (int64_t)(hctl[0].cands + hctl[1].cands);
+                    stats->leaves += (int64_t)(hctl[0].leaves + hctl[1].leaves);
+                    stats->points += (int64_t)npts;
+                    stats->donated += (int64_t)(hctl[0].donated + hctl[1].donated);
+                    stats->fp64_retries += (int64_t)retries;
+                }
+                if (in->verbose)
+                    fprintf(stderr, "pfg: batch @%lld: %d p | setup %.2f ms, search %.2f ms, output %.2f ms | "
+                                    "nodes %llu, points %llu -> %llu rows, donated %llu, fp64 retries %llu\n",
+                            (long long)off, nb, ms[0], ms[1], ms[2], hctl[0].nodes + hctl[1].nodes, npts, n_out,
+                            hctl[0].donated + hctl[1].donated, retries);
+            }
+            off += nb;
+        }
+    }
+    {
+        const size_t n = qo.size();
+        out->n = (int64_t)n;
+        out->M = (int64_t *)malloc(n * MH * 8 + 8);
+        out->Kn = (int64_t *)malloc(n * MH * 8 + 8);
+        out->q = (int64_t *)malloc(n * 8 + 8);
+        out->pidx = (int64_t *)malloc(n * 8 + 8);
+        if (!out->M || !out->Kn || !out->q || !out->pidx) { set_err(out, "out of host memory"); rc = 1; goto fail; }
+        if (n) {
+            memcpy(out->M, Mo.data(), n * MH * 8);
+            memcpy(out->Kn, Ko.data(), n * MH * 8);
+            memcpy(out->q, qo.data(), n * 8);
+            memcpy(out->pidx, po.data(), n * 8);
+        }
+    }
+fail:
+    for (auto &e : ev) if (e) cudaEventDestroy(e);
+    if (rc) {
+        cudaGetLastError();
+        pfg_output_free(out);
+    }
+    return rc;
+}

@@ -1,0 +1,146 @@
+// Exact integer helpers for the device code: checked int128 arithmetic,
+// binary gcd with an early exit, floor division, extended Euclid.
+#pragma once
+#include <cstdint>
+
+typedef __int128 i128;
+typedef unsigned __int128 u128;
+
+#define PFG_HD __host__ __device__ __forceinline__
+
+// PFG_UNIFORM(v): v must be equal in all lanes of the warp (a warp-uniform
+// branch input).  Checked only under the test-suite's CPU warp emulator.
+#ifdef PFG_EMU
+#define PFG_UNIFORM(v) emu_uniform((long long)(v), __LINE__)
+#else
+#define PFG_UNIFORM(v) ((void)0)
+#endif
+
+namespace pfg {
+
+PFG_HD u128 uabs(i128 x) { return x < 0 ? (u128)0 - (u128)x : (u128)x; }
+PFG_HD uint64_t uabs64(int64_t x) { return x < 0 ? (uint64_t)0 - (uint64_t)x : (uint64_t)x; }
+
+// |x| < 2^63 and x != INT64_MIN (so negation and division by -1 are defined)
+PFG_HD bool fits64(i128 x) { return x <= (i128)INT64_MAX && x > (i128)INT64_MIN; }
+
+// a + b, a - b with overflow detection (true on overflow)
+PFG_HD bool add_ovf(i128 a, i128 b, i128 *r)
+{
+    i128 s = (i128)((u128)a + (u128)b);
+    *r = s;
+    return ((a >= 0) == (b >= 0)) && ((s >= 0) != (a >= 0));
+}
+PFG_HD bool sub_ovf(i128 a, i128 b, i128 *r)
+{
+    i128 s = (i128)((u128)a - (u128)b);
+    *r = s;
+    return ((a >= 0) != (b >= 0)) && ((s >= 0) != (a >= 0));
+}
+// a * b with overflow detection
+PFG_HD bool mul_ovf(i128 a, i128 b, i128 *r)
+{
+    u128 ua = uabs(a), ub = uabs(b);
+    const u128 lim = (u128)1 << 63;
+    if (ua < lim && ub < lim) { *r = a * b; return false; }
+    if (ua == 0 || ub == 0) { *r = 0; return false; }
+    if (ub > ((((u128)1) << 127) - 1) / ua) return true;
+    u128 m = ua * ub;
+    *r = ((a < 0) != (b < 0)) ? -(i128)m : (i128)m;
+    return false;
+}
+
+PFG_HD int ctz64(uint64_t x)
+{
+#ifdef __CUDA_ARCH__
+    return __ffsll((long long)x) - 1;
+#else
+    return __builtin_ctzll(x);
+#endif
+}
+PFG_HD int ctz128(u128 x)
+{
+    uint64_t lo = (uint64_t)x;
+    return lo ? ctz64(lo) : 64 + ctz64((uint64_t)(x >> 64));
+}
+
+// Stein's binary gcd
+PFG_HD uint64_t gcd64(uint64_t u, uint64_t v)
+{
+    if (u == 0) return v;
+    if (v == 0) return u;
+    int sh = ctz64(u | v);
+    u >>= ctz64(u);
+    do {
+        v >>= ctz64(v);
+        if (u > v) { uint64_t t = v; v = u; u = t; }
+        v -= u;
+    } while (v);
+    return u << sh;
+}
+
+// gcd(u, v) if it is >= need, else 0 (u, v not both 0): the odd part of the
+// gcd is at most min(u, v) after each step, so stop once that cannot reach need.
+PFG_HD uint64_t gcd64_ge(uint64_t u, uint64_t v, uint64_t need)
+{
+    if (u == 0) return v >= need ? v : 0;
+    if (v == 0) return u >= need ? u : 0;
+    int sh = ctz64(u | v);
+    uint64_t need_s = (need >> sh) + ((need & ((1ULL << sh) - 1)) != 0);
+    u >>= ctz64(u);
+    do {
+        v >>= ctz64(v);
+        if (u > v) { uint64_t t = v; v = u; u = t; }
+        if (u < need_s) return 0;
+        v -= u;
+    } while (v);
+    return u << sh;
+}
+
+PFG_HD u128 gcd128(u128 u, u128 v)
+{
+    if ((u >> 64) == 0 && (v >> 64) == 0) return gcd64((uint64_t)u, (uint64_t)v);
+    if (u == 0) return v;
+    if (v == 0) return u;
+    int sh = ctz128(u | v);
+    u >>= ctz128(u);
+    do {
+        v >>= ctz128(v);
+        if (u > v) { u128 t = v; v = u; u = t; }
+        v -= u;
+        if ((u >> 64) == 0 && (v >> 64) == 0)
+            return (u128)gcd64((uint64_t)u, (uint64_t)v) << sh;
+    } while (v);
+    return u << sh;
+}
+
+// floor division (Python //) for b != 0
+PFG_HD int64_t fdiv64(int64_t a, int64_t b)
+{
+    int64_t q = a / b;
+    if ((a % b != 0) && ((a < 0) != (b < 0))) q--;
+    return q;
+}
+PFG_HD i128 fdiv128(i128 a, i128 b)
+{
+    i128 q = a / b;
+    if ((a % b != 0) && ((a < 0) != (b < 0))) q--;
+    return q;
+}
+
+// Extended Euclid with floor division: s a + t b = g (the sign convention of
+// the reference's util.extended_euclidean / pfl_xgcd).
+PFG_HD int64_t xgcd_floor(int64_t a, int64_t b, int64_t *s, int64_t *t)
+{
+    int64_t r0 = a, r1 = b, s0 = 1, s1 = 0, t0 = 0, t1 = 1;
+    while (r1 != 0) {
+        int64_t q = fdiv64(r0, r1), x;
+        x = r0 - q * r1; r0 = r1; r1 = x;
+        x = s0 - q * s1; s0 = s1; s1 = x;
+        x = t0 - q * t1; t0 = t1; t1 = x;
+    }
+    *s = s0; *t = t0;
+    return r0;
+}
+
+}  // namespace pfg

@@ -1,0 +1,584 @@
+// The Fincke-Pohst search on the device: one warp per subtree.
+//
+// Semantics are those of the reference search fpk_search
+// (pfvs/fp_kernel/fpk_search_impl.h:217-455): c is set from its last
+// coordinate to its first; per level the candidate range comes from the
+// ellipsoid radius widened by a rigorous rounding-error bound, narrowed by
+// the GCD bound of the rows already determined and, at the M0 level, by the
+// exact interval M0 = g_lin c[d-1] >= M0min; each candidate is tested on the
+// ellipsoid (with the error term en), exactly on M0, and on the GCD cut with
+// an early-exit gcd; leaves are decided exactly (q in int128, gcd of
+// Kn[1:] = (ZB c)[1:] exactly).  Floating point only prunes.
+//
+// B200 mapping.  The 32 lanes of a warp share one DFS: lane l keeps the
+// state of levels l and l+32 in registers (candidate range, remaining norm,
+// error bound, centre offset, gcd of the rows above, the GCD row's prefix,
+// and c[l]); entering a level is a warp-wide dot product (lane j multiplies
+// U[i][j] c[j]) reduced with shuffles; the 32 lanes test 32 sibling
+// candidates at once and a ballot picks the next child (DFS order) or the
+// passing leaves.  The exact sums mat c and ZB c are kept per lane
+// (lane r owns rows r, r+32) and updated by one column whenever a coordinate
+// changes, so a leaf costs O(1) exact work.  (M = Binter c is formed after
+// the search from the emitted c.)  Warps take whole directions
+// from a counter and donate the top of their DFS stack to a global queue
+// when other warps run out of work (persistent kernel, work stealing).
+#pragma once
+#include "pfg_types.cuh"
+
+namespace pfg {
+
+struct WorkItem {                 // an entered node with its remaining candidates
+    int32_t pid, level;
+    int64_t cur, hi;
+    double rem, err;
+    uint64_t glo, ghi;            // gcd of the rows above (u128)
+    int32_t c[MD + 1];            // c[level+1 .. d-1]
+};
+
+struct SearchCtl {
+    unsigned roots_next;          // next index into the todo list
+    unsigned q_tail, q_head;      // queue reservation / consumption
+    int active;                   // warps holding work
+    int err;                      // first error (ST_WAIT) if any
+    int pad;
+    unsigned long long npts;      // points emitted by all passes (see SearchArgs::npts)
+    unsigned long long nodes, cands, leaves, donated;
+};
+
+struct SearchArgs {
+    const Geo *geo;
+    Dir *dirs;
+    const int64_t *slab;
+    const int32_t *todo;          // directions to search (their status is ST_PENDING)
+    int n_todo;
+    int pass;                     // written into each point (stale passes are dropped)
+    SearchCtl *ctl;
+    WorkItem *items;
+    int *ready;
+    unsigned q_cap;
+    PointHdr *hdr;
+    int32_t *coords;              // (cap, MD)
+    unsigned long long pts_cap;
+    unsigned long long *npts;     // points emitted (shared by all passes; may exceed pts_cap)
+    unsigned long long *dir_nodes;  // per direction
+    double eps;
+    int donate;                   // 0: the plain form (no queue)
+    int n_warps;                  // warps of the persistent grid
+    long long wait_ns;            // bound on idle waiting (globaltimer ns)
+    long long deadline_ns;        // bound on one subtree's search (globaltimer ns)
+};
+
+__device__ __forceinline__ unsigned long long gtimer()
+{
+#ifdef PFG_EMU
+    return emu_now_ns();
+#else
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+#endif
+}
+
+template <class T> __device__ __forceinline__ T shfl(T x, int src) { return __shfl_sync(FULL, x, src); }
+__device__ __forceinline__ i128 shfl128(i128 x, int src)
+{
+    long long lo = (long long)(uint64_t)x, hi = (long long)(x >> 64);
+    lo = __shfl_sync(FULL, lo, src);
+    hi = __shfl_sync(FULL, hi, src);
+    return (i128)(((u128)(uint64_t)hi << 64) | (uint64_t)lo);
+}
+__device__ __forceinline__ u128 shflu128(u128 x, int src) { return (u128)shfl128((i128)x, src); }
+__device__ __forceinline__ i128 warp_sum128(i128 x)
+{
+    for (int o = 16; o; o >>= 1) {
+        long long lo = (long long)(uint64_t)x, hi = (long long)(x >> 64);
+        lo = __shfl_xor_sync(FULL, lo, o);
+        hi = __shfl_xor_sync(FULL, hi, o);
+        x += (i128)(((u128)(uint64_t)hi << 64) | (uint64_t)lo);
+    }
+    return x;
+}
+template <class R> __device__ __forceinline__ R warp_sumr(R x)
+{
+    for (int o = 16; o; o >>= 1) x += __shfl_xor_sync(FULL, x, o);
+    return x;
+}
+
+template <class R> struct Num;
+template <> struct Num<float> {
+    static __device__ float U() { return 0x1p-24f; }
+    static __device__ float G() { return 64 * 0x1p-24f; }
+    static __device__ float tiny() { return 1e-30f; }
+    static __device__ float i32max() { return 2147483520.0f; }
+};
+template <> struct Num<double> {
+    static __device__ double U() { return 0x1p-53; }
+    static __device__ double G() { return 1e-9; }
+    static __device__ double tiny() { return 1e-300; }
+    static __device__ double i32max() { return 2147483647.0; }
+};
+
+template <class R> struct Prob {
+    const R *U, *UI;
+    const int64_t *H, *MAT, *BT, *ZT;
+    int d, h, m0_level, pad;
+    int64_t g_lin, Q, qmax, linmin;
+    uint64_t hrows;
+    R qmax_r, slack, Kerr, max_err;
+};
+
+template <class R> __device__ Prob<R> load_prob(const SearchArgs &A, int pid)
+{
+    const Dir D = A.dirs[pid];
+    const Geo g = A.geo[D.geo];
+    const Slab L = slab_layout(D.h, D.d);
+    const int64_t *s = A.slab + D.slab;
+    Prob<R> P;
+    P.d = D.d; P.h = D.h; P.m0_level = D.m0_level;
+    P.g_lin = D.g_lin; P.Q = g.Q; P.qmax = g.qmax; P.linmin = g.linmin; P.hrows = D.hrows;
+    if (sizeof(R) == 4) { P.U = (const R *)(s + L.u32); P.UI = (const R *)(s + L.ui32); }
+    else { P.U = (const R *)(s + L.u64); P.UI = (const R *)(s + L.ui64); }
+    P.H = s + L.H; P.MAT = s + L.mat; P.BT = s + L.bt; P.ZT = s + L.zt;
+    const R qd = (R)g.qmax;
+    P.qmax_r = qd;
+    // search constants (fpk_search_impl.h:30-39), plus the certified margin
+    // of the FP64 Cholesky factor
+    R sl = (R)A.eps > Num<R>::G() * (qd + (R)1) ? (R)A.eps : Num<R>::G() * (qd + (R)1);
+    P.slack = sl + (R)D.slack_chol;
+    P.Kerr = (R)2 * (R)(D.d + 8) * Num<R>::U();
+    P.max_err = sizeof(R) < sizeof(double) ? (R)1 + (R)0.05 * qd : (R)INFINITY;
+    return P;
+}
+
+// smallest gcd that can pass the GCD cut when q >= q_lb (fpk_search_impl.h:43-51)
+template <class R> __device__ __forceinline__ uint64_t need_of(R q_lb, int64_t Q)
+{
+    if (!(q_lb > 0)) return 0;
+    R t = q_lb / (R)Q;
+    t -= Num<R>::G() * ((R)1 + t);
+    if (t < 0) t = 0;
+    if (t >= (R)1.8e19) return UINT64_MAX;
+    return (uint64_t)floor((double)t) + 1;             // strict cut
+}
+// the branch must fail Q g > q when q >= q_lb (fpk_search_impl.h:56-62)
+template <class R> __device__ __forceinline__ bool gcd_fails(u128 g, int64_t Q, R q_lb)
+{
+    if (g == 0 || (g >> 64) != 0) return false;
+    R Qg = (R)Q * (R)(uint64_t)g;
+    return Qg <= q_lb;
+}
+
+struct Tally { unsigned long long nodes, cands, leaves; };
+
+// Per-lane register state: levels lane (slot 0) and lane + 32 (slot 1).
+template <class R> struct Lanes {
+    int64_t cur0, cur1, hi0, hi1;
+    R rem0, rem1, err0, err1, off0, off1, aoff0, aoff1;
+    u128 gab0, gab1;              // gcd of the rows above the level
+    i128 pre0, pre1;              // GCD-row prefix at the level
+    int32_t c0, c1;               // c[lane], c[lane+32]
+    int64_t y0, y1;               // (mat c)_r, r = lane, lane+32, over c[1:]
+    int64_t k0, k1;               // (ZB c)_r over c[1:]
+};
+
+#define LGET(S, f, i) shfl((i) < 32 ? S.f##0 : S.f##1, (i) & 31)
+#define LSET(S, f, i, val) do { if (lane == ((i) & 31)) { if ((i) < 32) S.f##0 = (val); else S.f##1 = (val); } } while (0)
+
+// c[i] changes by dv (i >= 1): update the exact incremental sums
+template <class R> __device__ __forceinline__ void apply_dc(Lanes<R> &S, const Prob<R> &P, int i, int64_t dv, int lane)
+{
+    if (dv == 0 || i == 0) return;
+    const int d = P.d, h = P.h;
+    if (lane < d) S.y0 += P.MAT[i * d + lane] * dv;
+    if (lane + 32 < d) S.y1 += P.MAT[i * d + lane + 32] * dv;
+    if (lane < h) S.k0 += P.ZT[i * h + lane] * dv;
+    if (lane + 32 < h) S.k1 += P.ZT[i * h + lane + 32] * dv;
+}
+
+// the dot products of entering level i (c[i+1:] set): off, aoff, GCD prefix
+template <class R> __device__ __forceinline__ void level_sums(const Lanes<R> &S, const Prob<R> &P, int i, int lane,
+                                                              R &off, R &aoff, i128 &pre)
+{
+    const int d = P.d;
+    R o = 0, a = 0;
+    i128 pr = 0;
+    const bool hrow = (P.hrows >> i) & 1;
+    int j = lane;
+    if (j > i && j < d) {
+        R t = P.U[i * d + j] * (R)S.c0;
+        o += t; a += fabs(t);
+        if (hrow) pr += (i128)P.H[i * d + j] * S.c0;
+    }
+    j = lane + 32;
+    if (j > i && j < d) {
+        R t = P.U[i * d + j] * (R)S.c1;
+        o += t; a += fabs(t);
+        if (hrow) pr += (i128)P.H[i * d + j] * S.c1;
+    }
+    off = warp_sumr(o);
+    aoff = warp_sumr(a);
+    pre = hrow ? warp_sum128(pr) : (i128)0;
+}
+
+// Enter level i: candidate range [lo, hi] (lo > hi: none).  Returns
+// ST_RANGE if a bound leaves int32.
+template <class R> __device__ int enter_level(Lanes<R> &S, const Prob<R> &P, int i, R rem, R err, u128 gab,
+                                              int lane, int64_t &lo_o, int64_t &hi_o)
+{
+    R off, aoff;
+    i128 pre;
+    level_sums(S, P, i, lane, off, aoff, pre);
+    const R slack = P.slack, Kerr = P.Kerr;
+    R Rr = sqrt(fmax(rem + slack + err, (R)0));
+    Rr += Kerr * (Rr + (R)2 * aoff) + Num<R>::tiny();
+    bool empty = false;
+    if (gab != 0 && (gab >> 64) == 0) {                 // GCD narrowing
+        R am = Rr + (R)2 * aoff;
+        R Rg2 = (R)P.Q * (R)(uint64_t)gab - (P.qmax_r - rem) + slack + err + Kerr * (am * am + rem);
+        if (Rg2 < (R)0) empty = true;
+        else {
+            R Rg = sqrt(Rg2);
+            Rg += Kerr * (Rg + (R)2 * aoff) + Num<R>::tiny();
+            if (Rg < Rr) Rr = Rg;
+        }
+    }
+    int64_t lo = 1, hi = 0;
+    if (!empty) {
+        const R ui = P.UI[i];
+        R a = (-Rr - off) * ui, b = (Rr - off) * ui;
+        a = ceil(a - Num<R>::G() * ((R)1 + fabs(a)));
+        b = floor(b + Num<R>::G() * ((R)1 + fabs(b)));
+        if (!(a >= -Num<R>::i32max() && b <= Num<R>::i32max())) return ST_RANGE;
+        lo = (int64_t)a; hi = (int64_t)b;
+        if (i == P.m0_level) {                          // exact M0 interval: g_lin v >= linmin
+            const i128 need = (i128)P.linmin, l = P.g_lin;
+            if (l > 0) {
+                i128 bnd = need >= 0 ? (need + l - 1) / l : -((-need) / l);
+                if (bnd > lo) lo = bnd > hi ? hi + 1 : (int64_t)bnd;
+            } else {
+                i128 nl = -l;
+                i128 bnd = need <= 0 ? (-need) / nl : -((need + nl - 1) / nl);
+                if (bnd < hi) hi = bnd < lo ? lo - 1 : (int64_t)bnd;
+            }
+        }
+    }
+    LSET(S, cur, i, lo); LSET(S, hi, i, hi);
+    LSET(S, rem, i, rem); LSET(S, err, i, err);
+    LSET(S, off, i, off); LSET(S, aoff, i, aoff);
+    LSET(S, gab, i, gab); LSET(S, pre, i, pre);
+    lo_o = lo; hi_o = hi;
+    return 0;
+}
+
+// exact leaf data of the level-0 node (c[1:] set): q(c) = A0 + 2 c0 B0 + m00 c0^2
+template <class R> __device__ __forceinline__ void leaf_data(const Lanes<R> &S, const Prob<R> &P, int lane,
+                                                             i128 &A0, int64_t &B0)
+{
+    i128 part = 0;
+    if (lane >= 1 && lane < P.d) part += (i128)S.c0 * S.y0;
+    if (lane + 32 < P.d) part += (i128)S.c1 * S.y1;
+    A0 = warp_sum128(part);
+    B0 = shfl(S.y0, 0);
+}
+
+template <class R>
+__device__ int run_subtree(const SearchArgs &A, const Prob<R> &P, int pid, const WorkItem *it, Tally &T, int lane)
+{
+    const int d = P.d, h = P.h;
+    Lanes<R> S;
+    S.cur0 = S.cur1 = 0; S.hi0 = S.hi1 = -1;
+    S.rem0 = S.rem1 = S.err0 = S.err1 = S.off0 = S.off1 = S.aoff0 = S.aoff1 = 0;
+    S.gab0 = S.gab1 = 0; S.pre0 = S.pre1 = 0;
+    S.c0 = S.c1 = 0; S.y0 = S.y1 = S.k0 = S.k1 = 0;
+    int top, i;
+    if (!it) {                                    // the root of the direction
+        top = i = d - 1;
+        int64_t lo, hi;
+        int st = enter_level(S, P, i, P.qmax_r, P.Kerr * P.qmax_r, (u128)0, lane, lo, hi);
+        if (st) return st;
+        T.nodes++;
+    } else {                                      // a donated node
+        top = i = it->level;
+        if (lane > i && lane < d) S.c0 = it->c[lane];
+        if (lane + 32 > i && lane + 32 < d) S.c1 = it->c[lane + 32];
+        // exact incremental sums from scratch
+        for (int j = i + 1; j < d; ++j) {
+            int32_t cj = shfl(j < 32 ? S.c0 : S.c1, j & 31);
+            apply_dc(S, P, j, cj, lane);
+        }
+        R off, aoff;
+        i128 pre;
+        level_sums(S, P, i, lane, off, aoff, pre);
+        const u128 gab = ((u128)it->ghi << 64) | it->glo;
+        LSET(S, cur, i, it->cur); LSET(S, hi, i, it->hi);
+        LSET(S, rem, i, (R)it->rem); LSET(S, err, i, (R)it->err);
+        LSET(S, off, i, off); LSET(S, aoff, i, aoff);
+        LSET(S, gab, i, gab); LSET(S, pre, i, pre);
+    }
+    const R slack = P.slack, Kerr = P.Kerr;
+    // leaf data for the current level-0 node: q(v) = A0 + 2 v B0 + m00 v^2
+    i128 A0 = 0;
+    int64_t B0 = 0;
+    if (i == 0) leaf_data(S, P, lane, A0, B0);
+    const int64_t m00 = P.MAT[0];
+    unsigned poll = 0;
+    const unsigned long long t0 = shfl(gtimer(), 0);
+    for (;;) {
+        if (i > top) break;
+        int64_t cur = LGET(S, cur, i), hi = LGET(S, hi, i);
+        if (cur > hi) {                           // backtrack
+            int32_t ci = LGET(S, c, i);
+            if (ci) { apply_dc(S, P, i, -(int64_t)ci, lane); LSET(S, c, i, 0); }
+            ++i;
+            continue;
+        }
+        // donate the top of the stack when other warps are idle
+        if (((++poll) & 4095) == 0 && (long long)(shfl(gtimer(), 0) - t0) > A.deadline_ns)
+            return ST_WAIT;                       // (uniform: lane 0's clock)
+        if (A.donate && (poll & 63) == 0) {
+            int hungry = 0;
+            if (lane == 0) {
+                volatile SearchCtl *C = A.ctl;
+                const int queued = (int)(C->q_tail - C->q_head);
+                hungry = C->roots_next >= (unsigned)A.n_todo && queued < A.n_warps - C->active;
+            }
+            hungry = shfl(hungry, 0);
+            if (hungry) {
+                // highest level j in (i, top] with candidates left
+                bool has0 = lane > i && lane <= top && S.cur0 <= S.hi0;
+                bool has1 = lane + 32 > i && lane + 32 <= top && S.cur1 <= S.hi1;
+                unsigned b1 = __ballot_sync(FULL, has1), b0 = __ballot_sync(FULL, has0);
+                int j = b1 ? 32 + 31 - __clz(b1) : (b0 ? 31 - __clz(b0) : -1);
+                if (j >= 0) {
+                    unsigned slot = 0;
+                    if (lane == 0) slot = atomicAdd(&A.ctl->q_tail, 1u);
+                    slot = shfl(slot, 0);
+                    if (slot < A.q_cap) {
+                        WorkItem *dst = A.items + slot;
+                        const int64_t jc = LGET(S, cur, j), jh = LGET(S, hi, j);
+                        const R jr = LGET(S, rem, j), je = LGET(S, err, j);
+                        const u128 jg = shflu128(j < 32 ? S.gab0 : S.gab1, j & 31);
+                        if (lane == 0) {
+                            dst->pid = pid; dst->level = j; dst->cur = jc; dst->hi = jh;
+                            dst->rem = (double)jr; dst->err = (double)je;
+                            dst->glo = (uint64_t)jg; dst->ghi = (uint64_t)(jg >> 64);
+                        }
+                        if (lane > j && lane < d) dst->c[lane] = S.c0;
+                        if (lane + 32 > j && lane + 32 < d) dst->c[lane + 32] = S.c1;
+                        __threadfence();
+                        __syncwarp();
+                        if (lane == 0) { atomicExch(&A.ready[slot], 1); atomicAdd(&A.ctl->donated, 1ull); }
+                        LSET(S, hi, j, jc - 1);
+                    }
+                }
+            }
+        }
+        const R rem = LGET(S, rem, i), err = LGET(S, err, i), off = LGET(S, off, i), aoff = LGET(S, aoff, i);
+        const u128 gab = shflu128(i < 32 ? S.gab0 : S.gab1, i & 31);
+        const i128 pre = shfl128(i < 32 ? S.pre0 : S.pre1, i & 31);
+        const bool hrow = (P.hrows >> i) & 1;
+        const int64_t hii = hrow ? P.H[i * d + i] : 0;
+        const R uii = P.U[i * d + i];
+        const int64_t ncand = min((int64_t)32, hi - cur + 1);
+        const int64_t v = cur + lane;
+        bool pass = lane < ncand;
+        R nr = 0, en = 0;
+        u128 gn = gab;
+        bool ferr = false;
+        if (pass) {
+            R x = uii * (R)v + off;
+            nr = rem - x * x;
+            R ai = fabs(uii * (R)v) + aoff;
+            en = err + Kerr * (ai * ai + rem);
+            if (en > P.max_err) { ferr = true; pass = false; }
+            else if (nr < -(slack + en)) pass = false;
+        }
+        if (pass && i == P.m0_level && (i128)P.g_lin * v < (i128)P.linmin) pass = false;
+        if (pass) {
+            const R q_lb = (P.qmax_r - nr) - (slack + en);
+            if (hrow) {
+                if (gcd_fails(gn, P.Q, q_lb)) pass = false;
+                else {
+                    u128 a = uabs(pre + (i128)hii * v);
+                    if ((gn >> 64) == 0 && (a >> 64) == 0 && (gn | a) != 0) {
+                        uint64_t gg = gcd64_ge((uint64_t)gn, (uint64_t)a, need_of(q_lb, P.Q));
+                        if (!gg) pass = false;
+                        gn = gg;
+                    } else {
+                        gn = gcd128(gn, a);
+                    }
+                }
+            }
+            if (pass && gcd_fails(gn, P.Q, q_lb)) pass = false;
+        }
+        if (__any_sync(FULL, ferr)) return ST_FLOAT;
+        T.cands += (unsigned long long)ncand;
+        unsigned mask = __ballot_sync(FULL, pass);
+        if (i > 0) {
+            if (!mask) { LSET(S, cur, i, cur + ncand); continue; }
+            const int t0 = __ffs(mask) - 1;
+            const int64_t vc = cur + t0;
+            LSET(S, cur, i, vc + 1);
+            const R nr0 = shfl(nr, t0), en0 = shfl(en, t0);
+            const u128 g0 = shflu128(gn, t0);
+            const int32_t ci = LGET(S, c, i);
+            apply_dc(S, P, i, vc - ci, lane);
+            LSET(S, c, i, (int32_t)vc);
+            --i;
+            int64_t lo, hh;
+            int st = enter_level(S, P, i, nr0, en0, g0, lane, lo, hh);
+            if (st) return st;
+            T.nodes++;
+            if (i == 0) leaf_data(S, P, lane, A0, B0);
+            continue;
+        }
+        // leaves: exact q, exact gcd of Kn[1:], emission
+        LSET(S, cur, i, cur + ncand);
+        if (!mask) continue;
+        T.leaves += __popc(mask);
+        bool ok = pass;
+        i128 q = 0;
+        if (ok) {
+            q = A0 + (i128)2 * v * B0 + (i128)m00 * v * v;
+            if (q > (i128)P.qmax) ok = false;
+        }
+        unsigned need_g = __ballot_sync(FULL, ok && q >= (i128)P.Q);
+        while (need_g) {                          // Q g > q needs g = gcd(Kn[1:]) exactly
+            const int t = __ffs(need_g) - 1;
+            need_g &= need_g - 1;
+            const int64_t vt = cur + t;
+            const i128 qt = shfl128(q, t);
+            uint64_t g = 0;
+            if (lane >= 1 && lane < h) g = gcd64(g, uabs64(S.k0 + P.ZT[lane] * vt));
+            if (lane + 32 < h) g = gcd64(g, uabs64(S.k1 + P.ZT[lane + 32] * vt));
+            for (int o = 16; o; o >>= 1) g = gcd64(g, __shfl_xor_sync(FULL, g, o));
+            if (g != 0 && (i128)P.Q * (i128)g <= qt && lane == t) ok = false;
+        }
+        unsigned emit = __ballot_sync(FULL, ok);
+        if (!emit) continue;
+        unsigned long long base = 0;
+        if (lane == 0) base = atomicAdd(A.npts, (unsigned long long)__popc(emit));
+        base = __shfl_sync(FULL, base, 0);
+        unsigned e2 = emit;
+        for (unsigned k = 0; e2; ++k) {
+            const int t = __ffs(e2) - 1;
+            e2 &= e2 - 1;
+            const unsigned long long slot = base + k;
+            if (slot >= A.pts_cap) continue;
+            const int64_t vt = cur + t;
+            const i128 qt = shfl128(q, t);
+            if (lane == 0) {
+                A.hdr[slot].pid = pid;
+                A.hdr[slot].pad = A.pass;
+                A.hdr[slot].q = (int64_t)qt;
+            }
+            int32_t *cc = A.coords + slot * MD;
+            if (lane == 0) cc[0] = (int32_t)vt;
+            else if (lane < d) cc[lane] = S.c0;
+            if (lane + 32 < d) cc[lane + 32] = S.c1;
+        }
+    }
+    return 0;
+}
+
+template <class R>
+__device__ void finish_item(const SearchArgs &A, int pid, int st, Tally &T, int lane)
+{
+    if (lane == 0) {
+        atomicAdd(&A.dir_nodes[pid], T.nodes);
+        atomicAdd(&A.ctl->nodes, T.nodes);
+        atomicAdd(&A.ctl->cands, T.cands);
+        atomicAdd(&A.ctl->leaves, T.leaves);
+        if (st) atomicCAS(&A.dirs[pid].status, ST_PENDING, st);
+    }
+    T.nodes = T.cands = T.leaves = 0;
+}
+
+// Persistent batched search: warps take directions from the todo list, then
+// donated nodes from the queue; all bounded waits report ST_WAIT.
+template <class R>
+__global__ void __launch_bounds__(256) k_search(SearchArgs A)
+{
+    const int lane = threadIdx.x & 31;
+    Tally T{0, 0, 0};
+    const unsigned long long t_start = gtimer();
+    for (;;) {
+        int pid = -1;
+        const WorkItem *it = nullptr;
+        int got = 0;                              // 1 root, 2 queue item
+        if (lane == 0) {
+            volatile SearchCtl *C = A.ctl;
+            for (;;) {
+                // 'active' counts warps holding work; idle warps only read it.
+                // A warp raises it just before grabbing an item it has seen,
+                // and a worker pushes its donations before lowering it.
+                if (C->roots_next < (unsigned)A.n_todo) {
+                    atomicAdd(&A.ctl->active, 1);
+                    unsigned r = atomicAdd(&A.ctl->roots_next, 1u);
+                    if (r < (unsigned)A.n_todo) { got = 1; pid = A.todo[r]; break; }
+                    atomicSub(&A.ctl->active, 1);
+                }
+                unsigned head = C->q_head, tail = C->q_tail;
+                if (tail > A.q_cap) tail = A.q_cap;
+                if (head < tail) {
+                    atomicAdd(&A.ctl->active, 1);
+                    if (atomicCAS(&A.ctl->q_head, head, head + 1) == head) {
+                        volatile int *rd = A.ready + head;
+                        long long spins = 0;
+                        while (*rd == 0 && spins < (1LL << 22)) { __nanosleep(64); ++spins; }
+                        __threadfence();
+                        if (*rd) { got = 2; it = A.items + head; pid = it->pid; break; }
+                        atomicCAS(&A.ctl->err, 0, ST_WAIT);     // a reserved slot never filled
+                        atomicSub(&A.ctl->active, 1);
+                        break;
+                    }
+                    atomicSub(&A.ctl->active, 1);
+                    continue;
+                }
+                // finished when nobody holds work and, after that, nothing is queued
+                if (C->active == 0) {
+                    __threadfence();
+                    unsigned h2 = C->q_head, t2 = C->q_tail;
+                    if (t2 > A.q_cap) t2 = A.q_cap;
+                    if (h2 >= t2 && C->roots_next >= (unsigned)A.n_todo) break;
+                }
+                if ((long long)(gtimer() - t_start) > A.wait_ns || C->err) {
+                    atomicCAS(&A.ctl->err, 0, ST_WAIT);
+                    break;
+                }
+                __nanosleep(256);
+            }
+        }
+        got = shfl(got, 0);
+        if (!got) break;
+        pid = shfl(pid, 0);
+        unsigned long long ip = shfl((unsigned long long)it, 0);
+        it = (const WorkItem *)ip;
+        int st = 0;
+        int pending = 0;
+        if (lane == 0) pending = ((volatile Dir *)A.dirs)[pid].status == ST_PENDING;
+        if (shfl(pending, 0)) {                   // (skip work of a direction that already failed)
+            const Prob<R> P = load_prob<R>(A, pid);
+            st = run_subtree<R>(A, P, pid, it, T, lane);
+        }
+        finish_item<R>(A, pid, st, T, lane);
+        __threadfence();
+        if (lane == 0) atomicSub(&A.ctl->active, 1);
+    }
+}
+
+// The plain form: one direction per launch, one warp, no work sharing.
+template <class R>
+__global__ void __launch_bounds__(32) k_search_plain(SearchArgs A, int pid)
+{
+    const int lane = threadIdx.x & 31;
+    Tally T{0, 0, 0};
+    int pending = 0;
+    if (lane == 0) pending = A.dirs[pid].status == ST_PENDING;
+    if (!shfl(pending, 0)) return;
+    const Prob<R> P = load_prob<R>(A, pid);
+    int st = run_subtree<R>(A, P, pid, nullptr, T, lane);
+    finish_item<R>(A, pid, st, T, lane);
+}
+
+}  // namespace pfg

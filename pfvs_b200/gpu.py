@@ -1,0 +1,259 @@
+"""
+The B200 backend of the batched coni pipeline, loaded with ctypes -- the
+same module interface as the reference's `pfvs.gpu` (pfvs/gpu.py:26-232):
+`available`, `unavailable_reason`, `backend`, `release`, `max_h11`,
+`coni_batch_multi`, `coni_batch`.  The library is libpfvs_gpu.so next to
+this module (pfvs_b200/fp_kernel/) or the file named by PFVS_GPU_LIB, as
+the reference looks it up (pfvs/gpu.py:57-82).
+
+Differences from the reference backend (all within its contract): every
+direction is finished on the device -- `pstat` is 0, or a negative kernel
+status (-8 coordinates beyond int32, -9 not positive definite, -20 exact
+values beyond the device's integers, -21 FP64 factor not certified) that
+`coniZpM` turns into IncompleteSearchError; never 1 ("redo on the CPU").
+`coni_batch_multi_ex` adds the search form, the pruning precision and
+statistics.
+"""
+import ctypes
+import glob
+import math
+import os
+
+import numpy as np
+
+_i64p = ctypes.POINTER(ctypes.c_int64)
+_i32p = ctypes.POINTER(ctypes.c_int32)
+
+FORM_BATCHED, FORM_PLAIN = 0, 1
+PREC_AUTO, PREC_FP64, PREC_FP32 = 0, 1, 2
+
+
+class _Input(ctypes.Structure):
+    _fields_ = [("n_geo", ctypes.c_int), ("h", _i32p),
+                ("Q", _i64p), ("qmax", _i64p), ("linmin", _i64p),
+                ("kappa", _i64p), ("Mbasis", _i64p),
+                ("n_p", ctypes.c_int64), ("ps", _i64p), ("pgeo", _i32p),
+                ("device", ctypes.c_int), ("batch", ctypes.c_int64),
+                ("verbose", ctypes.c_int)]
+
+
+class _Output(ctypes.Structure):
+    _fields_ = [("n", ctypes.c_int64), ("M", _i64p), ("Kn", _i64p),
+                ("q", _i64p), ("pidx", _i64p),
+                ("pstat", ctypes.POINTER(ctypes.c_int8)),
+                ("seconds_gpu", ctypes.c_double), ("err", ctypes.c_char * 256)]
+
+
+class _Options(ctypes.Structure):
+    _fields_ = [("form", ctypes.c_int), ("precision", ctypes.c_int),
+                ("blocks_per_sm", ctypes.c_int), ("warps_per_block", ctypes.c_int)]
+
+
+class _Stats(ctypes.Structure):
+    _fields_ = [("nodes", ctypes.c_int64), ("candidates", ctypes.c_int64),
+                ("leaves", ctypes.c_int64), ("points", ctypes.c_int64),
+                ("donated", ctypes.c_int64), ("fp64_retries", ctypes.c_int64),
+                ("ms_setup", ctypes.c_double), ("ms_search", ctypes.c_double),
+                ("ms_output", ctypes.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+_lib = None
+_lib_error = None
+LIB_DIR = os.path.join(os.path.dirname(os.path.abspath(__file__)), "fp_kernel")
+
+
+def library_path():
+    """The shared library this module loads (PFVS_GPU_LIB, else the in-tree build)."""
+    path = os.environ.get("PFVS_GPU_LIB")
+    if path:
+        return path
+    found = sorted(glob.glob(os.path.join(LIB_DIR, "libpfvs_gpu*.so")))
+    return found[0] if found else None
+
+
+def _load():
+    global _lib, _lib_error
+    if _lib is not None or _lib_error is not None:
+        return _lib
+    path = library_path()
+    if not path:
+        _lib_error = ("the B200 backend was not built (python -c 'import pfvs_b200.build as b; "
+                      "b.build()', or __graft_entry__.build())")
+        return None
+    try:
+        lib = ctypes.CDLL(path)
+    except OSError as e:
+        _lib_error = f"could not load {path}: {e}"
+        return None
+    lib.pfg_max_h11.restype = ctypes.c_int
+    lib.pfg_backend.restype = ctypes.c_char_p
+    lib.pfg_device_count.restype = ctypes.c_int
+    lib.pfg_coni_batch.argtypes = [ctypes.POINTER(_Input), ctypes.POINTER(_Output)]
+    lib.pfg_coni_batch.restype = ctypes.c_int
+    lib.pfg_coni_batch_ex.argtypes = [ctypes.POINTER(_Input), ctypes.POINTER(_Options),
+                                      ctypes.POINTER(_Output), ctypes.POINTER(_Stats), _i64p]
+    lib.pfg_coni_batch_ex.restype = ctypes.c_int
+    lib.pfg_output_free.argtypes = [ctypes.POINTER(_Output)]
+    lib.pfg_release.argtypes = [ctypes.c_int]
+    _lib = lib
+    return lib
+
+
+def _require():
+    lib = _load()
+    if lib is None:
+        raise RuntimeError(_lib_error)
+    return lib
+
+
+def available() -> bool:
+    """Whether the backend is built and a CUDA device is present
+    (pfvs/gpu.py:85-95)."""
+    lib = _load()
+    return lib is not None and lib.pfg_device_count() > 0
+
+
+def unavailable_reason() -> str:
+    """Why `available()` is False ('' if it is True)."""
+    lib = _load()
+    if lib is None:
+        return _lib_error
+    if lib.pfg_device_count() == 0:
+        return "no CUDA device found"
+    return ""
+
+
+def backend() -> str:
+    """'cuda'."""
+    return _require().pfg_backend().decode()
+
+
+def release(device: int = 0) -> None:
+    """Free the device buffers kept between calls on `device`."""
+    lib = _load()
+    if lib is not None:
+        lib.pfg_release(int(device))
+
+
+def max_h11() -> int:
+    """The largest h11 the build supports (64)."""
+    return _require().pfg_max_h11()
+
+
+def _qmax(Q, dilation):
+    return int(math.floor(dilation * Q + 1e-7))
+
+
+def _pack(geoms, ps, pgeo, MH):
+    n_geo = len(geoms)
+    h = np.array([np.asarray(g["kappa"]).shape[0] for g in geoms], dtype=np.int32)
+    if n_geo and (h.min() < 3 or h.max() > MH):
+        raise ValueError(f"the GPU build supports 3 <= h11 <= {MH}")
+    Q = np.array([int(g["Q"]) for g in geoms], dtype=np.int64)
+    qmax = np.array([_qmax(int(g["Q"]), g["dilation"]) for g in geoms], dtype=np.int64)
+    linmin = np.array([math.ceil(g["M0min"] - 1e-9) for g in geoms], dtype=np.int64)
+    kap = np.concatenate([np.ascontiguousarray(g["kappa"], dtype=np.int64).ravel() for g in geoms]) \
+        if n_geo else np.zeros(1, dtype=np.int64)
+    Mb = np.concatenate([np.ascontiguousarray(g["Mbasis"], dtype=np.int64).ravel() for g in geoms]) \
+        if n_geo else np.zeros(1, dtype=np.int64)
+    pgeo = np.ascontiguousarray(pgeo, dtype=np.int32)
+    n_p = len(pgeo)
+    P = np.zeros((max(n_p, 1), MH), dtype=np.int64)
+    if isinstance(ps, np.ndarray) and ps.ndim == 2:
+        P[:n_p, :ps.shape[1]] = ps
+    else:
+        for i, p in enumerate(ps):
+            P[i, :len(p)] = p
+    if n_p and (np.any(pgeo < 0) or np.any(pgeo >= n_geo)):
+        raise ValueError("pgeo: geometry index out of range")
+    if n_p and np.any(P[:n_p][np.arange(MH)[None, :] >= h[pgeo][:, None]] != 0):
+        raise ValueError("a p-vector is longer than its geometry's h11")
+    return h, Q, qmax, linmin, kap, Mb, P, pgeo, n_p
+
+
+def coni_batch_multi_ex(geoms, ps, pgeo, device=0, batch=0, verbose=False,
+                        form=FORM_BATCHED, precision=PREC_AUTO, blocks_per_sm=0,
+                        warps_per_block=0, want_dir_nodes=False):
+    """
+    `coni_batch_multi` with the search form (FORM_BATCHED: one persistent
+    work-stealing launch; FORM_PLAIN: one launch per direction), the pruning
+    precision (PREC_AUTO: FP32 where qmax < 2^22 with an FP64 retry on -11;
+    PREC_FP64) and the call's statistics.  Returns
+    (M, Kn, q, pidx, pstat, seconds_gpu, stats dict[, dir_nodes]).
+    """
+    lib = _require()
+    MH = lib.pfg_max_h11()
+    h, Q, qmax, linmin, kap, Mb, P, pgeo, n_p = _pack(geoms, ps, pgeo, MH)
+    inp = _Input(len(geoms), h.ctypes.data_as(_i32p), Q.ctypes.data_as(_i64p),
+                 qmax.ctypes.data_as(_i64p), linmin.ctypes.data_as(_i64p),
+                 kap.ctypes.data_as(_i64p), Mb.ctypes.data_as(_i64p),
+                 n_p, P.ctypes.data_as(_i64p), pgeo.ctypes.data_as(_i32p),
+                 int(device), int(batch), int(bool(verbose)))
+    opt = _Options(int(form), int(precision), int(blocks_per_sm), int(warps_per_block))
+    st = _Stats()
+    dn = np.zeros(max(n_p, 1), dtype=np.int64)
+    out = _Output()
+    rc = lib.pfg_coni_batch_ex(ctypes.byref(inp), ctypes.byref(opt), ctypes.byref(out),
+                               ctypes.byref(st), dn.ctypes.data_as(_i64p))
+    if rc != 0:
+        raise RuntimeError(f"GPU pipeline failed: {out.err.decode(errors='replace')}")
+    try:
+        n = out.n
+
+        def arr(ptr, shape):
+            if n == 0:
+                return np.zeros(shape, dtype=np.int64)
+            return np.ctypeslib.as_array(ptr, shape=shape).copy()
+        M, Kn = arr(out.M, (n, MH)), arr(out.Kn, (n, MH))
+        q, pidx = arr(out.q, (n,)), arr(out.pidx, (n,))
+        pstat = np.ctypeslib.as_array(out.pstat, shape=(n_p,)).copy() if n_p \
+            else np.zeros(0, dtype=np.int8)
+        secs = out.seconds_gpu
+    finally:
+        lib.pfg_output_free(ctypes.byref(out))
+    res = (M, Kn, q, pidx, pstat.astype(np.int8), secs, st.as_dict())
+    return res + (dn[:n_p],) if want_dir_nodes else res
+
+
+def coni_batch_multi(geoms, ps, pgeo, device=0, batch=0, verbose=False):
+    """
+    The batched coni pipeline on the GPU for p-vectors of several geometries
+    at once (pfvs/gpu.py:136-211).
+
+    - `geoms`: per geometry a dict with `kappa` (h, h, h), `Mbasis` (h, h),
+      `Q`, `dilation`, `M0min`.
+    - `ps`: the p-vectors, each of length h of its geometry, *with* the
+      leading 0.
+    - `pgeo`: the geometry index of each p-vector.
+
+    Returns (M, Kn, q, pidx, pstat, seconds_gpu): for every lattice point
+    M = Binter c and Kn = Z Binter c (rows of width max_h11(), first h
+    entries valid), q = c^T mat c, its p-vector index; points grouped by
+    p-vector (ascending), sorted by (M, Kn) within one.
+    """
+    return coni_batch_multi_ex(geoms, ps, pgeo, device, batch, verbose)[:6]
+
+
+def coni_batch(kappa, Mbasis, ps, Q, dilation, M0min, max_N_out, device=0):
+    """
+    One geometry (pfvs/gpu.py:214-232): (M, Kn, q, pidx, pstat), rows cut to
+    h columns.  A p-vector with more than max_N_out points gets pstat -2
+    ("more than max_N_pfvs outputs", as the reference kernel's status) and
+    none of its points are returned.
+    """
+    kappa = np.asarray(kappa)
+    h = kappa.shape[0]
+    ps = np.asarray(ps, dtype=np.int64)
+    geoms = [dict(kappa=kappa, Mbasis=Mbasis, Q=Q, dilation=dilation, M0min=M0min)]
+    M, Kn, q, pidx, pstat, _ = coni_batch_multi(geoms, ps, np.zeros(len(ps), dtype=np.int32),
+                                                device=device)
+    counts = np.bincount(pidx, minlength=len(ps)) if len(pidx) else np.zeros(len(ps), dtype=np.int64)
+    over = counts > max_N_out
+    if np.any(over):
+        pstat[over] = -2
+        keep = ~over[pidx]
+        M, Kn, q, pidx = M[keep], Kn[keep], q[keep], pidx[keep]
+    return M[:, :h], Kn[:, :h], q, pidx, pstat

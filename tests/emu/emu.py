@@ -1,0 +1,68 @@
+"""TEST INFRASTRUCTURE: ctypes wrapper for tests/emu/_build/libpfvs_emu.so
+(the library's device kernels run on CPU threads under warp_emu.h)."""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(HERE, "_build", "libpfvs_emu.so")
+SRCS = [os.path.join(HERE, f) for f in ("emu_driver.cpp", "warp_emu.h")] + [
+    os.path.join(HERE, "..", "..", "pfvs_b200", "csrc", f) for f in
+    ("pfg_int.cuh", "pfg_types.cuh", "pfg_setup.cuh", "pfg_search.cuh", "pfg_out.cuh")] + [
+    os.path.join(HERE, "..", "..", "include", "pfvs_gpu.h")]
+_lib = None
+
+
+def build():
+    os.makedirs(os.path.dirname(LIB), exist_ok=True)
+    if os.path.exists(LIB) and all(os.path.getmtime(s) <= os.path.getmtime(LIB) for s in SRCS):
+        return
+    subprocess.run(["g++", "-std=c++20", "-O1", "-g", "-pthread", "-shared", "-fPIC", "-w",
+                    os.path.join(HERE, "emu_driver.cpp"), "-o", LIB], check=True)
+
+
+def _load():
+    global _lib
+    if _lib is None:
+        build()
+        from pfvs_b200 import gpu
+        lib = ctypes.CDLL(LIB)
+        lib.emu_coni_batch.argtypes = [ctypes.POINTER(gpu._Input), ctypes.c_int, ctypes.c_int,
+                                       ctypes.POINTER(gpu._Output), ctypes.POINTER(ctypes.c_int64),
+                                       ctypes.POINTER(ctypes.c_int32)]
+        lib.emu_coni_batch.restype = ctypes.c_int
+        lib.emu_output_free.argtypes = [ctypes.POINTER(gpu._Output)]
+        _lib = lib
+    return _lib
+
+
+def coni_batch_multi(geoms, ps, pgeo, precision=0, n_warps=2):
+    """As pfvs_b200.gpu.coni_batch_multi, on the emulated warps.  Returns
+    (M, Kn, q, pidx, pstat, dir_nodes, setup_failure_stage)."""
+    from pfvs_b200 import gpu
+    lib = _load()
+    MH = 64
+    h, Q, qmax, linmin, kap, Mb, P, pgeo, n_p = gpu._pack(geoms, ps, pgeo, MH)
+    i64p, i32p = ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int32)
+    inp = gpu._Input(len(geoms), h.ctypes.data_as(i32p), Q.ctypes.data_as(i64p),
+                     qmax.ctypes.data_as(i64p), linmin.ctypes.data_as(i64p),
+                     kap.ctypes.data_as(i64p), Mb.ctypes.data_as(i64p), n_p,
+                     P.ctypes.data_as(i64p), pgeo.ctypes.data_as(i32p), 0, 0, 0)
+    out = gpu._Output()
+    dn = np.zeros(max(n_p, 1), np.int64)
+    dbg = np.zeros(max(n_p, 1), np.int32)
+    rc = lib.emu_coni_batch(ctypes.byref(inp), int(precision), int(n_warps), ctypes.byref(out),
+                            dn.ctypes.data_as(i64p), dbg.ctypes.data_as(i32p))
+    if rc:
+        raise RuntimeError(out.err.decode())
+    try:
+        n = out.n
+        arr = (lambda p, s: np.ctypeslib.as_array(p, shape=s).copy() if n else np.zeros(s, np.int64))
+        M, Kn = arr(out.M, (n, MH)), arr(out.Kn, (n, MH))
+        q, pidx = arr(out.q, (n,)), arr(out.pidx, (n,))
+        pstat = np.ctypeslib.as_array(out.pstat, shape=(n_p,)).copy()
+    finally:
+        lib.emu_output_free(ctypes.byref(out))
+    return M, Kn, q, pidx, pstat, dn[:n_p], dbg[:n_p]

@@ -1,0 +1,140 @@
+// TEST INFRASTRUCTURE -- never part of the product.
+//
+// Runs the library's device kernels (pfvs_b200/csrc/*.cuh, compiled for the
+// host against warp_emu.h) on CPU threads, in the same sequence as the
+// library's host code (pfvs_b200/csrc/pfg_abi.cu): setup, FP32 search,
+// flip, FP64 search, expand/count/scan/scatter/segsort/gather.  Exposed as
+// emu_coni_batch() with the pfg_input/pfg_output structs, for CPU tests of
+// the device logic and for debugging without a GPU.  Not loadable by the
+// product (the product loads only libpfvs_gpu*.so).
+#define PFG_EMU 1
+#include "warp_emu.h"
+
+#include <cstdio>
+#include <cstdlib>
+#include <vector>
+
+#include "../../include/pfvs_gpu.h"
+#include "../../pfvs_b200/csrc/pfg_int.cuh"
+#include "../../pfvs_b200/csrc/pfg_types.cuh"
+#include "../../pfvs_b200/csrc/pfg_setup.cuh"
+#include "../../pfvs_b200/csrc/pfg_search.cuh"
+#include "../../pfvs_b200/csrc/pfg_out.cuh"
+
+using namespace pfg;
+
+template <class K> static void launch(unsigned grid, K kernel)
+{
+    for (unsigned b = 0; b < grid; ++b) emu_run_warp(b, 0, 32, grid, kernel);
+}
+
+extern "C" int emu_coni_batch(const pfg_input *in, int precision, int n_warps, pfg_output *out,
+                              int64_t *dir_nodes_out, int32_t *dir_debug)
+{
+    memset(out, 0, sizeof *out);
+    const int64_t NP = in->n_p;
+    std::vector<Geo> geos(in->n_geo);
+    int64_t koff = 0, moff = 0;
+    for (int gi = 0; gi < in->n_geo; ++gi) {
+        Geo &g = geos[gi];
+        g.h = in->h[gi]; g.d = g.h - 1;
+        g.Q = in->Q[gi]; g.qmax = in->qmax[gi]; g.linmin = in->linmin[gi];
+        g.use_f32 = g.qmax < (1LL << 22) && precision != PFG_PREC_FP64;
+        g.koff = koff; g.moff = moff;
+        g.slab_len = slab_layout(g.h, g.d).len;
+        koff += (int64_t)g.h * g.h * g.h;
+        moff += (int64_t)g.h * g.h;
+    }
+    out->pstat = (int8_t *)calloc(NP > 0 ? NP : 1, 1);
+    const int nb = (int)NP;
+    std::vector<int64_t> slab_off(nb);
+    std::vector<int32_t> todo32, todoall(nb), pgeo(in->pgeo, in->pgeo + nb);
+    int64_t slab_total = 0;
+    for (int k = 0; k < nb; ++k) {
+        slab_off[k] = slab_total;
+        slab_total += geos[pgeo[k]].slab_len;
+        todoall[k] = k;
+        if (geos[pgeo[k]].use_f32) todo32.push_back(k);
+    }
+    std::vector<int64_t> slab(slab_total + 1);
+    std::vector<Dir> dirs(nb);
+    const int setup_warps = 4;
+    std::vector<SetupScratch> scratch(setup_warps);
+    unsigned next = 0;
+    SetupArgs SA{geos.data(), in->kappa, in->Mbasis, in->ps, pgeo.data(), slab_off.data(), slab.data(),
+                 dirs.data(), scratch.data(), nb, &next};
+    fprintf(stderr, "emu: setup\n");
+    launch(setup_warps, [&] { k_setup(SA); });
+    fprintf(stderr, "emu: setup done\n");
+
+    const unsigned long long pts_cap = 1 << 20;
+    const unsigned q_cap = 1 << 14;
+    std::vector<SearchCtl> ctl(2);
+    memset(ctl.data(), 0, 2 * sizeof(SearchCtl));
+    std::vector<WorkItem> items(q_cap);
+    std::vector<int> ready(q_cap, 0);
+    std::vector<PointHdr> hdr(pts_cap);
+    std::vector<int32_t> coords((size_t)pts_cap * MD);
+    std::vector<unsigned long long> dnodes(nb, 0), retries(1, 0);
+    std::vector<int32_t> dpass(nb, 1);
+    SearchArgs A{};
+    A.geo = geos.data(); A.dirs = dirs.data(); A.slab = slab.data(); A.items = items.data();
+    A.ready = ready.data(); A.q_cap = q_cap; A.hdr = hdr.data(); A.coords = coords.data();
+    A.pts_cap = pts_cap; A.npts = &ctl[0].npts; A.dir_nodes = dnodes.data(); A.eps = 1e-4;
+    A.donate = 1; A.n_warps = n_warps; A.wait_ns = 30ll * 1000000000ll; A.deadline_ns = 600ll * 1000000000ll;
+    if (!todo32.empty()) {
+        A.ctl = &ctl[0]; A.todo = todo32.data(); A.n_todo = (int)todo32.size(); A.pass = 1;
+        launch(n_warps, [&] { k_search<float>(A); });
+    }
+    for (int pid = 0; pid < nb; ++pid) {          // k_flip
+        Dir &D = dirs[pid];
+        if (!geos[D.geo].use_f32) continue;
+        if (D.status == ST_PENDING) D.status = ST_OK;
+        else if (D.status == ST_FLOAT) { D.status = ST_PENDING; dpass[pid] = 2; retries[0]++; }
+    }
+    std::fill(ready.begin(), ready.end(), 0);
+    A.ctl = &ctl[1]; A.todo = todoall.data(); A.n_todo = nb; A.pass = 2;
+    launch(n_warps, [&] { k_search<double>(A); });
+    if (ctl[0].err || ctl[1].err) { snprintf(out->err, sizeof out->err, "wait ran out"); return 1; }
+    const unsigned long long npts = ctl[0].npts;
+    if (npts > pts_cap) { snprintf(out->err, sizeof out->err, "point buffer overflow"); return 1; }
+    std::vector<int64_t> Mf(std::max<unsigned long long>(npts, 1) * MH), Kf(std::max<unsigned long long>(npts, 1) * MH);
+    std::vector<int> derr(nb, 0);
+    std::vector<unsigned> cnt(nb, 0), fill(nb, 0), idx(std::max<unsigned long long>(npts, 1)), pad(2 * std::max<unsigned long long>(npts, 1) + 64);
+    std::vector<unsigned long long> seg(nb + 1, 0);
+    OutArgs O{dirs.data(), slab.data(), hdr.data(), coords.data(), dpass.data(), npts, nb, Mf.data(), Kf.data(),
+              derr.data(), cnt.data(), fill.data(), seg.data(), idx.data()};
+    if (npts) {
+        launch(4, [&] { k_expand(O); });
+        launch(4, [&] { k_count(O); });
+    }
+    launch(1, [&] { k_scan(O); });
+    if (npts) {
+        launch(4, [&] { k_scatter(O); });
+        launch(std::min(nb, 8), [&] { k_segsort(O, pad.data()); });
+    }
+    const unsigned long long n_out = seg[nb];
+    out->n = (int64_t)n_out;
+    out->M = (int64_t *)malloc(n_out * MH * 8 + 8);
+    out->Kn = (int64_t *)malloc(n_out * MH * 8 + 8);
+    out->q = (int64_t *)malloc(n_out * 8 + 8);
+    out->pidx = (int64_t *)malloc(n_out * 8 + 8);
+    if (n_out) {
+        GatherArgs G{idx.data(), hdr.data(), Mf.data(), Kf.data(), n_out, 0, out->M, out->Kn, out->q, out->pidx};
+        launch(4, [&] { k_gather(G); });
+    }
+    for (int k = 0; k < nb; ++k) {
+        int st = dirs[k].status;
+        if (derr[k]) st = ST_OVERFLOW;
+        out->pstat[k] = (st == ST_OK || st == ST_PENDING || st == ST_EMPTY) ? 0 : (int8_t)st;
+        if (dir_nodes_out) dir_nodes_out[k] = (int64_t)dnodes[k];
+        if (dir_debug) dir_debug[k] = dirs[k].pad;
+    }
+    return 0;
+}
+
+extern "C" void emu_output_free(pfg_output *out)
+{
+    free(out->M); free(out->Kn); free(out->q); free(out->pidx); free(out->pstat);
+    memset(out, 0, sizeof *out);
+}

@@ -1,0 +1,84 @@
+"""
+GPU parity of the batched coniZpM pipeline: the B200 library's points
+(M, Kn, q, pidx, in the canonical order) equal the oracle's -- this
+repository's CPU restatement -- and the reference's own CPU kernel
+(oracle/_ref) element for element, on seeded synthetic workloads, in both
+search forms and both pruning precisions (as the reference's
+tests/test_gpu.py:51-81 compares its GPU and CPU arrays).
+"""
+import numpy as np
+import pytest
+
+from pfvs_b200 import gpu, workloads
+from parity import assert_same, expected, layout
+
+pytestmark = pytest.mark.gpu
+
+CASES = [
+    ("small", 256, None),
+    ("small", 128, (150.0,)),
+    ("small", 64, (800.0,)),
+    ("plain", 256, None),
+    ("plain", 96, (150.0,)),
+    ("mixed", 256, None),
+    ("precision", 24, None),
+    ("large", 6, None),
+]
+
+
+@pytest.fixture(scope="module", autouse=True)
+def _built(lib):
+    if not gpu.available():
+        pytest.fail("no CUDA device: " + gpu.unavailable_reason())
+
+
+def _ids(c):
+    return f"{c[0]}-{c[1]}-dil{'x'.join(str(int(d)) for d in c[2]) if c[2] else 'cfg'}"
+
+
+@pytest.mark.parametrize("case", CASES, ids=[_ids(c) for c in CASES])
+def test_batched_matches_oracle(case):
+    name, n, dils = case
+    w = workloads.build(name, n_p=n, dilations=dils)
+    geoms, ps, pgeo, hs = layout(w)
+    got = gpu.coni_batch_multi(geoms, ps, pgeo)
+    M, Kn, q, pidx, pstat, _ = got
+    assert np.all(pstat == 0), np.unique(pstat)
+    exp = expected(geoms, ps, pgeo, "oracle")
+    assert_same(got, exp)
+
+
+@pytest.mark.parametrize("case", CASES[:6], ids=[_ids(c) for c in CASES[:6]])
+def test_batched_matches_reference_build(case, ref_available):
+    if not ref_available:
+        pytest.skip("oracle/_ref not built")
+    name, n, dils = case
+    w = workloads.build(name, n_p=n, dilations=dils)
+    geoms, ps, pgeo, hs = layout(w)
+    got = gpu.coni_batch_multi(geoms, ps, pgeo)
+    exp = expected(geoms, ps, pgeo, "ref")
+    ok = exp[4] == 0            # (directions the reference's C path finished)
+    assert ok.mean() > 0.5
+    assert_same(got, exp, ok_mask=ok)
+
+
+@pytest.mark.parametrize("case", [CASES[2], CASES[4], CASES[5]], ids=_ids)
+def test_forms_and_precisions_agree(case):
+    name, n, dils = case
+    w = workloads.build(name, n_p=n, dilations=dils)
+    geoms, ps, pgeo, hs = layout(w)
+    a = gpu.coni_batch_multi_ex(geoms, ps, pgeo, precision=gpu.PREC_AUTO)
+    b = gpu.coni_batch_multi_ex(geoms, ps, pgeo, precision=gpu.PREC_FP64)
+    c = gpu.coni_batch_multi_ex(geoms, ps, pgeo, form=gpu.FORM_PLAIN, precision=gpu.PREC_FP64)
+    for x in (b, c):
+        assert_same(x, a)
+        np.testing.assert_array_equal(x[4], a[4])
+    assert a[6]["nodes"] > 0
+
+
+def test_repeat_calls_identical():
+    w = workloads.build("mixed", n_p=128)
+    geoms, ps, pgeo, _ = layout(w)
+    a = gpu.coni_batch_multi(geoms, ps, pgeo)
+    b = gpu.coni_batch_multi(geoms, ps, pgeo)
+    assert_same(b, a)
