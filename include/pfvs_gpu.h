@@ -96,6 +96,7 @@ typedef struct {
     int64_t donated;           /* subtrees handed between warps */
     int64_t fp64_retries;      /* directions re-searched in FP64 after -11 */
     double  ms_setup, ms_search, ms_output;   /* device time per stage */
+    int64_t launches;          /* kernels this library launched */
 } pfg_stats;
 
 /* pfg_coni_batch with options and statistics (opt, stats may be NULL);

@@ -30,13 +30,15 @@ using namespace pfg;
 
 namespace {
 
-// per-direction flip between the FP32 and FP64 passes
+// Between the FP32 and FP64 passes: an FP32-searched direction is done, or
+// (status -11) goes to the FP64 pass; every direction the FP64 pass will
+// search keeps only that pass's points (dir_pass = 2).
 __global__ void k_flip(Dir *dirs, const Geo *geo, int n, int f32_used, int32_t *dir_pass,
                        unsigned long long *retries)
 {
     for (int pid = blockIdx.x * blockDim.x + threadIdx.x; pid < n; pid += gridDim.x * blockDim.x) {
         Dir &D = dirs[pid];
-        if (!(f32_used && geo[D.geo].use_f32)) continue;
+        if (!(f32_used && geo[D.geo].use_f32)) { dir_pass[pid] = 2; continue; }
         if (D.status == ST_PENDING) D.status = ST_OK;
         else if (D.status == ST_FLOAT) { D.status = ST_PENDING; dir_pass[pid] = 2; atomicAdd(retries, 1ull); }
     }
@@ -177,6 +179,7 @@ extern "C" int pfg_coni_batch_ex(const pfg_input *in, const pfg_options *opt_in,
     if (NP == 0) return 0;
 
     int rc = 0;
+    int64_t launches = 0;
     Workspace &W = workspace(in->device);
     std::unique_lock<std::mutex> lock(W.mu);
     std::vector<int64_t> Mo, Ko, qo, po;
@@ -254,14 +257,14 @@ extern "C" int pfg_coni_batch_ex(const pfg_input *in, const pfg_options *opt_in,
             CK(cudaMemset(dctl, 0, 2 * sizeof(SearchCtl) + 64));
             CK(cudaMemset(ddirnodes, 0, (size_t)nb * 8));
             CK(cudaMemset(dretry, 0, 64));
-            k_fill_i32<<<(nb + 255) / 256, 256>>>(ddirpass, 1, nb);
+            k_fill_i32<<<(nb + 255) / 256, 256>>>(ddirpass, 1, nb); ++launches;
             CK(cudaGetLastError());
             // ---- setup ----
             CK(cudaEventRecord(ev[0]));
             {
                 SetupArgs SA{dgeo, dkappa, dmb, dps, dpgeo, dslaboff, dslab, ddirs, dscr, nb,
                              (unsigned *)((char *)dctl + 2 * sizeof(SearchCtl))};
-                k_setup<<<setup_warps / 4, 128>>>(SA);
+                k_setup<<<setup_warps / 4, 128>>>(SA); ++launches;
                 CK(cudaGetLastError());
             }
             CK(cudaEventRecord(ev[1]));
@@ -279,11 +282,11 @@ extern "C" int pfg_coni_batch_ex(const pfg_input *in, const pfg_options *opt_in,
                     A.ctl = dctl;
                     for (int k = 0; k < nb; ++k) {
                         const bool f32 = geos[in->pgeo[off + k]].use_f32;
-                        if (f32) k_search_plain<float><<<1, 32>>>(A, k);
+                        if (f32) { k_search_plain<float><<<1, 32>>>(A, k); ++launches; }
                     }
-                    k_flip<<<(nb + 255) / 256, 256>>>(ddirs, dgeo, nb, 1, ddirpass, dretry);
+                    k_flip<<<(nb + 255) / 256, 256>>>(ddirs, dgeo, nb, 1, ddirpass, dretry); ++launches;
                     A.pass = 2;
-                    for (int k = 0; k < nb; ++k) k_search_plain<double><<<1, 32>>>(A, k);
+                    for (int k = 0; k < nb; ++k) { k_search_plain<double><<<1, 32>>>(A, k); ++launches; }
                     CK(cudaGetLastError());
                 } else {
                     int bps = opt.blocks_per_sm;
@@ -298,14 +301,14 @@ extern "C" int pfg_coni_batch_ex(const pfg_input *in, const pfg_options *opt_in,
                     if (!todo32.empty()) {
                         A.ctl = dctl; A.todo = dtodo32; A.n_todo = (int)todo32.size(); A.pass = 1;
                         CK(cudaMemset(dready, 0, (size_t)q_cap * 4));
-                        k_search<float><<<grid, wpb * 32>>>(A);
+                        k_search<float><<<grid, wpb * 32>>>(A); ++launches;
                         CK(cudaGetLastError());
                     }
-                    k_flip<<<(nb + 255) / 256, 256>>>(ddirs, dgeo, nb, 1, ddirpass, dretry);
+                    k_flip<<<(nb + 255) / 256, 256>>>(ddirs, dgeo, nb, 1, ddirpass, dretry); ++launches;
                     // FP64 pass over everything still pending
                     A.ctl = dctl + 1; A.todo = dtodoall; A.n_todo = nb; A.pass = 2;
                     CK(cudaMemset(dready, 0, (size_t)q_cap * 4));
-                    k_search<double><<<grid, wpb * 32>>>(A);
+                    k_search<double><<<grid, wpb * 32>>>(A); ++launches;
                     CK(cudaGetLastError());
                 }
             }
@@ -339,13 +342,13 @@ extern "C" int pfg_coni_batch_ex(const pfg_input *in, const pfg_options *opt_in,
             CK(cudaEventRecord(ev[3]));
             OutArgs O{ddirs, dslab, dhdr, dcoords, ddirpass, npts, nb, dM, dK, derr, dcount, dfill, dseg, didx};
             if (npts) {
-                k_expand<<<nsm * 8, 256>>>(O);
-                k_count<<<nsm * 4, 256>>>(O);
+                k_expand<<<nsm * 8, 256>>>(O); ++launches;
+                k_count<<<nsm * 4, 256>>>(O); ++launches;
             }
-            k_scan<<<1, 1024>>>(O);
+            k_scan<<<1, 1024>>>(O); ++launches;
             if (npts) {
-                k_scatter<<<nsm * 4, 256>>>(O);
-                k_segsort<<<std::min(nb, nsm * 8), 256>>>(O, dpad);
+                k_scatter<<<nsm * 4, 256>>>(O); ++launches;
+                k_segsort<<<std::min(nb, nsm * 8), 256>>>(O, dpad); ++launches;
             }
             CK(cudaGetLastError());
             unsigned long long n_out = 0;
@@ -357,7 +360,7 @@ extern "C" int pfg_coni_batch_ex(const pfg_input *in, const pfg_options *opt_in,
             WS(op, W_OP, std::max<unsigned long long>(n_out, 1) * 8);
             if (n_out) {
                 GatherArgs G{didx, dhdr, dM, dK, n_out, off, oM, oK, oq, op};
-                k_gather<<<nsm * 8, 256>>>(G);
+                k_gather<<<nsm * 8, 256>>>(G); ++launches;
                 CK(cudaGetLastError());
             }
             CK(cudaEventRecord(ev[4]));
@@ -409,6 +412,7 @@ extern "C" int pfg_coni_batch_ex(const pfg_input *in, const pfg_options *opt_in,
                     stats->points += (int64_t)npts;
                     stats->donated += (int64_t)(hctl[0].donated + hctl[1].donated);
                     stats->fp64_retries += (int64_t)retries;
+                    stats->launches = launches;
                 }
                 if (in->verbose)
                     fprintf(stderr, "pfg: batch @%lld: %d p | setup %.2f ms, search %.2f ms, output %.2f ms | "

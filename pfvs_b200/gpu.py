@@ -54,7 +54,7 @@ class _Stats(ctypes.Structure):
                 ("leaves", ctypes.c_int64), ("points", ctypes.c_int64),
                 ("donated", ctypes.c_int64), ("fp64_retries", ctypes.c_int64),
                 ("ms_setup", ctypes.c_double), ("ms_search", ctypes.c_double),
-                ("ms_output", ctypes.c_double)]
+                ("ms_output", ctypes.c_double), ("launches", ctypes.c_int64)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

@@ -146,7 +146,7 @@ def sample_directions(geom, n, emax, rng, max_tries=None):
 SPECS = {
     "small":     ([(5, 60, 8, (1, 3), (1, 3))], 256, 6, (1,)),
     "plain":     ([(11, 120, 8, (1, 4), (1, 3))], 4096, 8, (1,)),
-    "mixed":     ([(h, 2 * h + 40, 8, (1, 4), (1, 3, 5, 7)) for h in (8, 16, 24, 32)],
+    "mixed":     ([(h, 2 * h + 40, 8, (1, 4), (1, 3, 5, 7, 9)) for h in (8, 16, 24, 32)],
                   65536, 10, (1, 2, 3, 4)),
     "precision": ([(40, 150, 8, (1, 4), (1, 3, 5, 7, 9, 11, 13, 15))], 16384, 12, (2,)),
     "large":     ([(60, 200, 70, (1, 5), (1,))], 4096, 16, (1,)),

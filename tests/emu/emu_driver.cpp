@@ -88,7 +88,7 @@ extern "C" int emu_coni_batch(const pfg_input *in, int precision, int n_warps, p
     }
     for (int pid = 0; pid < nb; ++pid) {          // k_flip
         Dir &D = dirs[pid];
-        if (!geos[D.geo].use_f32) continue;
+        if (!geos[D.geo].use_f32) { dpass[pid] = 2; continue; }
         if (D.status == ST_PENDING) D.status = ST_OK;
         else if (D.status == ST_FLOAT) { D.status = ST_PENDING; dpass[pid] = 2; retries[0]++; }
     }
