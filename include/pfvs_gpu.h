@@ -104,6 +104,40 @@ typedef struct {
 int pfg_coni_batch_ex(const pfg_input *in, const pfg_options *opt, pfg_output *out,
                       pfg_stats *stats, int64_t *dir_nodes);
 
+/*
+ * No counterpart in the reference.  The coni pipeline for ONE p-vector,
+ * for callers that cannot allocate device memory while they run (code in a
+ * framework that owns all device memory through its own pool or arena, such
+ * as an XLA custom call or a TensorRT plugin; work issued while a stream is
+ * being captured; a real-time path that may not block on the allocator).
+ * The call allocates nothing: no cudaMalloc/cudaFree, no host allocation.
+ *
+ * Inputs (device pointers): kappa (h^3), Mbasis (h^2, basis vectors as
+ * columns), p (h entries, p[0] = 0); scalars h (3..64), Q, qmax =
+ * floor(dilation Q), linmin = ceil(M0min).  Outputs (device pointers, the
+ * caller's): M and Kn (cap x 64 int64, rows as pfg_output's), q (cap),
+ * n_out (1 int64: the number of rows) and status (1 int32: 0 done, -2 more
+ * than cap or PFG_STATIC_MAX_POINTS points, else a status of pfg_output's
+ * pstat).  The rows are exactly pfg_coni_batch's rows for that p-vector, in
+ * the same order.  The work is queued on `stream` (a cudaStream_t, or NULL);
+ * the outputs are valid once it completes.  Returns 0 when queued, 1 on bad
+ * arguments (message on stderr): h outside 3..64, cap outside
+ * 0..PFG_STATIC_MAX_POINTS.
+ *
+ * The scratch (about 3 MB) is a static device array that every GPU loading
+ * this library holds until the process exits.  All calls share it: calls
+ * that overlap on the GPU (other streams, other host threads) race; issue
+ * them one after another.  Each call clears what must start at zero; the
+ * array otherwise keeps the last call's contents.  The first call on a
+ * device looks up the array's device address (cudaGetSymbolAddress) with
+ * that device current; make that first call before any stream capture.
+ */
+#define PFG_STATIC_MAX_POINTS 2048
+int pfg_coni_direction_static(int h, int64_t Q, int64_t qmax, int64_t linmin,
+                              const int64_t *kappa, const int64_t *Mbasis, const int64_t *p,
+                              int64_t cap, int64_t *M, int64_t *Kn, int64_t *q,
+                              int64_t *n_out, int32_t *status, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -7,11 +7,11 @@ import os
 import subprocess
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-SRC = os.path.join(HERE, "csrc", "pfg_abi.cu")
+SRCS = [os.path.join(HERE, "csrc", "pfg_abi.cu"), os.path.join(HERE, "csrc", "pfg_static.cu")]
 OUT = os.path.join(HERE, "fp_kernel", "libpfvs_gpu.so")
 DEPS = [os.path.join(HERE, "csrc", f) for f in
-        ("pfg_abi.cu", "pfg_int.cuh", "pfg_types.cuh", "pfg_setup.cuh", "pfg_search.cuh",
-         "pfg_out.cuh")] + [os.path.join(HERE, "..", "include", "pfvs_gpu.h")]
+        ("pfg_abi.cu", "pfg_static.cu", "pfg_int.cuh", "pfg_types.cuh", "pfg_setup.cuh",
+         "pfg_search.cuh", "pfg_out.cuh")] + [os.path.join(HERE, "..", "include", "pfvs_gpu.h")]
 
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
               "-shared", "-Xcompiler", "-fPIC"]
@@ -31,7 +31,7 @@ def build(force=False, verbose=False, extra=()):
         t = os.path.getmtime(OUT)
         if all(os.path.getmtime(d) <= t for d in DEPS if os.path.exists(d)):
             return OUT
-    cmd = [nvcc(), *NVCC_FLAGS, *extra, SRC, "-o", OUT]
+    cmd = [nvcc(), *NVCC_FLAGS, *extra, *SRCS, "-o", OUT]
     if verbose:
         print(" ".join(cmd))
     subprocess.run(cmd, check=True)
