@@ -1,0 +1,174 @@
+"""
+CPU tests (no GPU): the oracle pinned to the reference, the committed golden
+vectors, the device sources under the CPU warp emulator, and the workload
+generator's properties.
+
+- the restated kernel vs the reference's 219 kernel fixtures (812 cases;
+  tests/test_kernels.py:64-77 of the reference) -- needs the reference tree;
+- the restated pipeline vs the published PFV sets of the reference's dataset
+  geometries under the rule of tests/test_dataset.py:59-86 (h11 <= 5 here,
+  so that the CPU suite stays within minutes);
+- the restated pipeline vs the reference build (oracle/_ref) and vs the
+  golden vectors generated from it (tests/golden/make_golden.py).
+"""
+import gzip
+import json
+import os
+
+import numpy as np
+import pytest
+
+from conftest import REFERENCE, ROOT
+from oracle import pfo, postproc, pvecs, ref
+from parity import assert_same, expected, layout
+from pfvs_b200 import intlat, workloads
+
+FIXTURES = os.path.join(REFERENCE, "tests", "data", "fixtures.json.gz")
+needs_reference = pytest.mark.skipif(not os.path.exists(FIXTURES), reason="reference tree not present")
+needs_ref_build = pytest.mark.skipif(not ref.available(), reason="oracle/_ref not built")
+
+
+def _fixtures():
+    with gzip.open(FIXTURES) as f:
+        return json.load(f)
+
+
+@needs_reference
+def test_oracle_kernel_matches_reference_fixtures():
+    F = _fixtures()
+    n = 0
+    for k in F["kernel"]:
+        for dil, exp in k["expected"].items():
+            qmax = ref.qmax_of(k["Q"], float(dil))
+            pts, qs, st, _ = pfo.kernel(k["mat"], k["Q"], qmax, k["H"], k["linvec"],
+                                        ref.linmin_of(k["M0min"]), strict=True)
+            assert st == 0
+            assert [tuple(map(int, r)) for r in pts] == [tuple(c) for c in exp["pts"]]
+            assert [int(x) for x in qs] == exp["qs"]
+            n += 1
+    assert n == 812
+
+
+@needs_reference
+def test_reference_build_matches_reference_fixtures(ref_available):
+    if not ref_available:
+        pytest.skip("oracle/_ref not built")
+    F = _fixtures()
+    for k in F["kernel"][::7]:
+        for dil, exp in k["expected"].items():
+            pts, qs, st, _ = ref.kernel(k["mat"], k["Q"], ref.qmax_of(k["Q"], float(dil)), k["H"],
+                                        k["linvec"], ref.linmin_of(k["M0min"]), strict=True)
+            assert st == 0 and [tuple(map(int, r)) for r in pts] == [tuple(c) for c in exp["pts"]]
+
+
+def _cydata(g):
+    h = g["h11"]
+    kappa = np.zeros((h,) * 3, dtype=np.int64)
+    for i, j, k, v in g["kappa_coo"]:
+        for a, b, c in {(i, j, k), (i, k, j), (j, i, k), (j, k, i), (k, i, j), (k, j, i)}:
+            kappa[a, b, c] = v
+    Hc = np.array(g["H"], dtype=np.int64)
+    return kappa, Hc[np.any(Hc != 0, axis=1)]
+
+
+@needs_reference
+def test_oracle_pipeline_reproduces_dataset_pfvs():
+    F = _fixtures()
+    done = 0
+    for g in F["geometries"]:
+        h = g["h11"]
+        if h > 5:
+            continue
+        kappa, Hc = _cydata(g)
+        Mb = intlat.m_lattice(kappa, np.array(g["c2"]))
+        ps = pvecs.box_enum(g["B"], Hc)
+        Q = h + g["h21"] + 4
+        exp = {(tuple(K), tuple(M)) for K, M in zip(g["K"], g["M"])}
+        if len(ps) == 0:
+            assert exp == set()
+            continue
+        pfull = np.hstack([np.zeros((len(ps), 1), np.int64), ps])
+        M, Kn, q, pidx, st, _ = pfo.coni_batch(kappa, Mb, pfull, Q, g["D"], 13)
+        assert np.all(st == 0)
+        Ks, Ms, _ = postproc.pfvs_from_points(M, Kn, q, pidx, kappa, h, Q, 13)
+        got = {(tuple(int(x) for x in K), tuple(int(x) for x in m)) for K, m in zip(Ks, Ms)}
+        primitive = {KM for KM in got if np.gcd.reduce(np.array(KM[0][1:])) == 1}
+        assert exp <= got and primitive == exp
+        for K, m in got - exp:
+            assert np.gcd.reduce(np.array(K[1:])) >= 2
+            assert -int(np.dot(K, m)) == Q and m[0] >= 13
+        done += 1
+    assert done >= 10
+
+
+@needs_ref_build
+@pytest.mark.parametrize("name,n,dils", [("plain", 64, (150.0,)), ("mixed", 48, None),
+                                         ("precision", 4, None)])
+def test_oracle_matches_reference_build(name, n, dils):
+    w = workloads.build(name, n_p=n, dilations=dils)
+    geoms, ps, pgeo, _ = layout(w)
+    a = expected(geoms, ps, pgeo, "oracle")
+    b = expected(geoms, ps, pgeo, "ref")
+    assert_same(a, b, ok_mask=b[4] == 0)
+
+
+GOLDEN = sorted(f[:-4] for f in os.listdir(os.path.join(ROOT, "tests", "golden")) if f.endswith(".npz"))
+
+
+@pytest.mark.parametrize("key", GOLDEN)
+def test_oracle_matches_golden(key):
+    """The oracle against the reference build's committed answers."""
+    G = np.load(os.path.join(ROOT, "tests", "golden", key + ".npz"))
+    dils = tuple(G["dilations"].tolist()) or None
+    w = workloads.build(str(G["workload"]), n_p=int(G["n"]), dilations=dils)
+    geoms, ps, pgeo, _ = layout(w)
+    M, Kn, q, pidx, st = expected(geoms, ps, pgeo, "oracle")
+    ok = G["status"] == 0
+    h = G["M"].shape[1]
+    sel = ok[pidx] if len(pidx) else np.zeros(0, bool)
+    np.testing.assert_array_equal(pidx[sel], G["pidx"])
+    np.testing.assert_array_equal(q[sel], G["q"])
+    np.testing.assert_array_equal(M[sel][:, :h], G["M"])
+    np.testing.assert_array_equal(Kn[sel][:, :h], G["Kn"])
+
+
+def test_postproc_singular_mask():
+    A = np.array([[[1, 2], [2, 4]], [[1, 0], [0, 1]], [[3, 5], [6, 10]]], dtype=np.int64)
+    np.testing.assert_array_equal(postproc.singular_mask(A), [True, False, True])
+
+
+def test_m_lattice_properties():
+    for h, rows, ones, sw in [(5, 8, (1, 3), (1, 3)), (11, 8, (1, 4), (1, 3))]:
+        g = workloads.make_geometry(h, 2 * h + 40, rows, ones, sw, seed=3)
+        a, b = intlat.a_matrix(g.kappa), intlat.b_vector(g.c2)
+        Mb = g.Mbasis
+        assert np.all((a @ Mb) % 2 == 0) and np.all((b @ Mb) % 24 == 0)
+        # index of the lattice = number of residue classes of Z^h it keeps, by counting mod 24
+        det = abs(round(np.linalg.det(Mb.astype(float))))
+        rng = np.random.default_rng(0)
+        # every integer vector satisfying the congruences is in the lattice
+        for _ in range(50):
+            x = rng.integers(-5, 6, h)
+            M = 24 * x
+            coeff = np.linalg.solve(Mb.astype(float), M.astype(float))
+            assert np.allclose(coeff, np.round(coeff))
+        assert det > 0
+
+
+def test_workload_prefix_property():
+    a = workloads.build("mixed", n_p=64)
+    b = workloads.build("mixed", n_p=16)
+    for i in range(16):
+        assert np.array_equal(a.ps[i], b.ps[i]) and a.pgeo[i] == b.pgeo[i] and a.dil[i] == b.dil[i]
+    assert all(workloads.lorentzian_ok(a.geoms[a.pgeo[i]].kappa, a.ps[i]) for i in range(64))
+
+
+def test_device_code_under_warp_emulator():
+    """The library's device sources, run on CPU threads (tests/emu), equal the
+    oracle on a small case; divergent warp collectives abort the run."""
+    from emu import emu
+    w = workloads.build("plain", n_p=6, dilations=(150.0,))
+    geoms, ps, pgeo, _ = layout(w)
+    M, Kn, q, pidx, pstat, nodes, stage = emu.coni_batch_multi(geoms, ps, pgeo)
+    assert np.all(pstat == 0) and nodes.sum() > 0
+    assert_same((M, Kn, q, pidx), expected(geoms, ps, pgeo, "oracle"))
