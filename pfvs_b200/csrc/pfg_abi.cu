@@ -50,7 +50,7 @@ __global__ void k_fill_i32(int32_t *a, int32_t v, int n)
 }
 
 enum {
-    W_GEO, W_KAPPA, W_MB, W_PS, W_PGEO, W_SLABOFF, W_SLAB, W_DIRS, W_SCRATCH, W_TODO32, W_TODOALL,
+    W_GEO, W_KAPPA, W_MB, W_PS, W_PGEO, W_SLABOFF, W_SLAB, W_DIRS, W_SCRATCH, W_TODO32, W_TODOALL, W_ORDER,
     W_CTL, W_ITEMS, W_READY, W_HDR, W_COORDS, W_DIRNODES, W_DIRPASS, W_MFULL, W_KNFULL,
     W_DIRERR, W_COUNT, W_FILL, W_SEG, W_IDX, W_PAD, W_OM, W_OK, W_OQ, W_OP, W_RETRY, W_N
 };
@@ -112,6 +112,16 @@ void set_err(pfg_output *out, const char *fmt, ...)
 #define WS(ptr, slot, bytes) CK(ws_get(W, slot, (size_t)(bytes), (void **)&(ptr)))
 
 extern "C" int pfg_max_h11(void) { return MH; }
+
+#ifdef PFG_STAGE_CLOCKS
+// profiling build only: read (and zero) the setup's per-stage cycle counters
+extern "C" int pfg_debug_stage_cycles(unsigned long long *out)
+{
+    if (cudaMemcpyFromSymbol(out, pfg::pfg_stage_cycles, sizeof(unsigned long long) * 64) != cudaSuccess) return 1;
+    unsigned long long z[64] = {};
+    return cudaMemcpyToSymbol(pfg::pfg_stage_cycles, z, sizeof z) != cudaSuccess;
+}
+#endif
 extern "C" const char *pfg_backend(void) { return "cuda"; }
 
 extern "C" int pfg_device_count(void)
@@ -218,7 +228,7 @@ extern "C" int pfg_coni_batch_ex(const pfg_input *in, const pfg_options *opt_in,
         for (int64_t off = 0; off < NP;) {
             const int nb = (int)std::min<int64_t>(batch, NP - off);
             int64_t *dps; int32_t *dpgeo; int64_t *dslaboff, *dslab; Dir *ddirs; SetupScratch *dscr;
-            int32_t *dtodo32, *dtodoall; SearchCtl *dctl; WorkItem *ditems; int *dready;
+            int32_t *dtodo32, *dtodoall, *dorder; SearchCtl *dctl; WorkItem *ditems; int *dready;
             PointHdr *dhdr; int32_t *dcoords; unsigned long long *ddirnodes, *dretry; int32_t *ddirpass;
             std::vector<int64_t> slab_off(nb);
             std::vector<int32_t> todo32, todoall(nb);
@@ -229,7 +239,27 @@ extern "C" int pfg_coni_batch_ex(const pfg_input *in, const pfg_options *opt_in,
                 todoall[k] = k;
                 if (geos[in->pgeo[off + k]].use_f32) todo32.push_back(k);
             }
-            const int setup_warps = (std::min(nb, nsm * 8) + 3) / 4 * 4;   // whole blocks of 4 warps
+            // setup order: h11 <= 32 (shared-memory LLL) then the rest, each largest h11 first
+            std::vector<int32_t> order(nb);
+            for (int k = 0; k < nb; ++k) order[k] = k;
+            std::stable_sort(order.begin(), order.end(), [&](int32_t a, int32_t b) {
+                const int ha = geos[in->pgeo[off + a]].h, hb = geos[in->pgeo[off + b]].h;
+                if ((ha <= 32) != (hb <= 32)) return ha <= 32;
+                return ha > hb;
+            });
+            int n32 = 0;
+            while (n32 < nb && geos[in->pgeo[off + order[n32]]].h <= 32) ++n32;
+            const int n64 = nb - n32;
+            const size_t smem32 = sizeof(LllMem<32>);
+            int grid32 = 0, grid64 = 0;
+            if (n32) {
+                CK(cudaFuncSetAttribute(k_setup<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem32));
+                int bpsm = 0;
+                CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bpsm, k_setup<32>, 32, smem32));
+                grid32 = std::min(n32, nsm * std::max(1, bpsm));
+            }
+            if (n64) grid64 = std::min((n64 + 3) / 4, nsm * 2);
+            const int setup_warps = std::max(grid32, grid64 * 4);
             WS(dps, W_PS, (size_t)nb * MH * 8);
             WS(dpgeo, W_PGEO, (size_t)nb * 4);
             WS(dslaboff, W_SLABOFF, (size_t)nb * 8);
@@ -238,6 +268,7 @@ extern "C" int pfg_coni_batch_ex(const pfg_input *in, const pfg_options *opt_in,
             WS(dscr, W_SCRATCH, (size_t)setup_warps * sizeof(SetupScratch));
             WS(dtodo32, W_TODO32, (size_t)std::max<size_t>(todo32.size(), 1) * 4);
             WS(dtodoall, W_TODOALL, (size_t)nb * 4);
+            WS(dorder, W_ORDER, (size_t)nb * 4);
             WS(dctl, W_CTL, 2 * sizeof(SearchCtl) + 64);
             WS(ditems, W_ITEMS, (size_t)q_cap * sizeof(WorkItem));
             WS(dready, W_READY, (size_t)q_cap * 4);
@@ -250,6 +281,7 @@ extern "C" int pfg_coni_batch_ex(const pfg_input *in, const pfg_options *opt_in,
             if (!todo32.empty())
                 CK(cudaMemcpy(dtodo32, todo32.data(), todo32.size() * 4, cudaMemcpyHostToDevice));
             CK(cudaMemcpy(dtodoall, todoall.data(), (size_t)nb * 4, cudaMemcpyHostToDevice));
+            CK(cudaMemcpy(dorder, order.data(), (size_t)nb * 4, cudaMemcpyHostToDevice));
 
         restart_search:
             WS(dhdr, W_HDR, pts_cap * sizeof(PointHdr));
@@ -262,10 +294,19 @@ extern "C" int pfg_coni_batch_ex(const pfg_input *in, const pfg_options *opt_in,
             // ---- setup ----
             CK(cudaEventRecord(ev[0]));
             {
-                SetupArgs SA{dgeo, dkappa, dmb, dps, dpgeo, dslaboff, dslab, ddirs, dscr, nb,
-                             (unsigned *)((char *)dctl + 2 * sizeof(SearchCtl))};
-                k_setup<<<setup_warps / 4, 128>>>(SA); ++launches;
-                CK(cudaGetLastError());
+                unsigned *counters = (unsigned *)((char *)dctl + 2 * sizeof(SearchCtl));
+                if (n32) {
+                    SetupArgs SA{dgeo, dkappa, dmb, dps, dpgeo, dslaboff, dslab, ddirs, dscr, n32,
+                                 counters, dorder, 1};
+                    k_setup<32><<<grid32, 32, smem32>>>(SA); ++launches;
+                    CK(cudaGetLastError());
+                }
+                if (n64) {
+                    SetupArgs SA{dgeo, dkappa, dmb, dps, dpgeo, dslaboff, dslab, ddirs, dscr, n64,
+                                 counters + 1, dorder + n32, 0};
+                    k_setup<MH><<<grid64, 128>>>(SA); ++launches;
+                    CK(cudaGetLastError());
+                }
             }
             CK(cudaEventRecord(ev[1]));
             // ---- search ----

@@ -8,6 +8,15 @@ typedef unsigned __int128 u128;
 
 #define PFG_HD __host__ __device__ __forceinline__
 
+// Out-of-line device functions: the setup's reduction routines are called
+// from several stages, and one shared copy keeps the kernel's hot code small
+// enough for the instruction caches.
+#ifdef PFG_EMU
+#define PFG_NOINLINE
+#else
+#define PFG_NOINLINE __noinline__
+#endif
+
 // PFG_UNIFORM(v): v must be equal in all lanes of the warp (a warp-uniform
 // branch input).  Checked only under the test-suite's CPU warp emulator.
 #ifdef PFG_EMU

@@ -21,38 +21,105 @@
 //   (the reference rounds an exact GMP/int128 Bareiss factor; in FP64 the
 //   factor is exact for mat + dA, |dA| <= gamma_{d+1} |U^T||U|, and the
 //   search widens its slack by a bound on c^T dA c over the ellipsoid).
+//
+// The lattice reductions work on an LllMem<N> (rows of length <= N, the
+// exact Gram in int128 as a packed triangle, packed Gram-Schmidt data): for
+// h11 <= 32 it lives in shared memory (about 23 KB per warp), above that in
+// the warp's global scratch.
 #pragma once
 #include "pfg_types.cuh"
 
 namespace pfg {
 
+// ---------------------------------------------------------------------------
+// LLL working set of one warp.
+// ---------------------------------------------------------------------------
+template <int N> struct LllMem {
+    static constexpr int R = N + 1;             // N basis rows + one 'last' row
+    int64_t B[R * N];                           // rows, stride N
+    i128 G[R * (R + 1) / 2];                    // exact Gram, lower triangle packed (gix)
+    i128 T[R];                                  // a copied column of G / a temporary vector
+    double mu[R * (R - 1) / 2];                 // Gram-Schmidt coefficients mu(k, j), j < k (mix)
+    double bb[R], ibb[R];                       // squared Gram-Schmidt norms, their inverses
+    int64_t q[R];                               // size-reduction / elimination multipliers
+};
+
+PFG_HD int gix(int i, int j) { return i >= j ? ((i * (i + 1)) >> 1) + j : ((j * (j + 1)) >> 1) + i; }
+PFG_HD int mix(int k, int j) { return ((k * (k - 1)) >> 1) + j; }
+// packed lower-triangle index e -> (i, j), j <= i
+PFG_HD void tri_of(int e, int &i, int &j)
+{
+    int r = (int)((sqrt(8.0 * e + 1.0) - 1.0) * 0.5);
+    while (((r + 1) * (r + 2) >> 1) <= e) ++r;
+    while ((r * (r + 1) >> 1) > e) --r;
+    i = r;
+    j = e - ((r * (r + 1)) >> 1);
+}
+
+// Cold working arrays of one warp (global memory), plus an LllMem for the
+// h11 > 32 path.
 struct SetupScratch {
     int64_t Z[MH * MH];
-    int64_t B[(MH + 1) * MH];       // LLL rows (+ the 'last' row)
-    i128 G[(MH + 1) * (MH + 1)];    // exact Gram of B's rows
-    double mu[MH * MH];
-    double bb[MH + 1];
     int64_t V[MH * MH];             // unimodular transforms / temporaries
     int64_t S[MH * MH];
     double X[MH * MH];              // U^-1 for the certificate
-    i128 y[MH];
     int64_t w[MH], v[MH];
     int order[MH];
+    LllMem<MH> core;
 };
-
-constexpr int LDG = MH + 1;
 
 struct SetupArgs {
     const Geo *geo;
     const int64_t *kappa, *Mbasis, *ps;     // ps: (n, MH)
     const int32_t *pgeo;
-    const int64_t *slab_off;                // (n,) slab offset per direction
+    const int64_t *slab_off;                // slab offset per direction
     int64_t *slab;
     Dir *dirs;
     SetupScratch *scratch;                  // one per warp
-    int n;
+    int n;                                  // entries of todo
     unsigned *next;                         // work counter
+    const int32_t *todo;                    // directions to set up (null: 0..n-1)
+    int smem_core;                          // 1: the LllMem<32> lives in dynamic shared memory
 };
+
+// Per-stage cycle accounting of the setup, compiled in only with
+// -DPFG_STAGE_CLOCKS (a profiling build): lane 0 adds the clock64() cycles
+// spent in each stage to pfg_stage_cycles[stage & 31]; counters [32..34]
+// count LLL calls, swaps and size-reduction passes.
+#ifdef PFG_STAGE_CLOCKS
+__device__ unsigned long long pfg_stage_cycles[64];
+struct StageClock {
+    int &stage;
+    int lane;
+    long long t;
+    __device__ StageClock(int &s, int l) : stage(s), lane(l), t(0)
+    {
+#ifdef __CUDA_ARCH__
+        t = clock64();
+#endif
+    }
+    __device__ void mark(int s)
+    {
+#ifdef __CUDA_ARCH__
+        if (lane == 0) {
+            long long n = clock64();
+            atomicAdd(&pfg_stage_cycles[stage & 31], (unsigned long long)(n - t));
+            t = n;
+        }
+#endif
+        stage = s;
+    }
+    __device__ ~StageClock() { mark(stage); }
+};
+#define PFG_COUNT(i, v) do { if ((threadIdx.x & 31) == 0) atomicAdd(&pfg_stage_cycles[32 + (i)], (unsigned long long)(v)); } while (0)
+#else
+struct StageClock {
+    int &stage;
+    __device__ StageClock(int &s, int) : stage(s) {}
+    __device__ void mark(int s) { stage = s; }
+};
+#define PFG_COUNT(i, v) do { } while (0)
+#endif
 
 __device__ __forceinline__ double warp_sum(double x)
 {
@@ -62,176 +129,326 @@ __device__ __forceinline__ double warp_sum(double x)
 
 __device__ __forceinline__ bool warp_any(bool b) { return __any_sync(FULL, b); }
 
+__device__ __forceinline__ i128 shfl_xor_i128(i128 x, int m)
+{
+    uint64_t lo = (uint64_t)x;
+    long long hi = (long long)(x >> 64);
+    lo = __shfl_xor_sync(FULL, lo, m);
+    hi = __shfl_xor_sync(FULL, hi, m);
+    return (i128)(((u128)(uint64_t)hi << 64) | lo);
+}
+
+// acc -= q * g; true on overflow
+PFG_HD bool submul_ovf(i128 &acc, int64_t q, i128 g)
+{
+    i128 t;
+    if (mul_ovf((i128)q, g, &t)) return true;
+    return sub_ovf(acc, t, &acc);
+}
+
 // ---------------------------------------------------------------------------
-// Warp LLL (delta 0.99) on the m rows of B (length n, stride MH) with exact
-// Gram G (stride LDG) over M = m + has_last rows; row m is 'last', which is
-// size-reduced against the reduced rows at the end.  Float Gram-Schmidt
-// data (mu, bb) are recomputed from the exact Gram and only choose the
-// unimodular steps.  Returns 0, or ST_OVERFLOW on an int64/int128 overflow
-// or rank loss, or when the iteration budget runs out.
+// Warp LLL (Schnorr-Euchner style) on the m rows of B (length n) with the
+// exact Gram over M = m + has_last rows; row m is 'last', size-reduced
+// against the reduced rows at the end.  Row and Gram updates are exact
+// (checked int64 / int128); the FP64 Gram-Schmidt data only choose the
+// unimodular steps and are recomputed from the exact Gram whenever a row is
+// visited.  Returns 0, or ST_OVERFLOW on an int64/int128 overflow, a
+// non-positive Gram-Schmidt norm, or when the iteration budget runs out.
 // ---------------------------------------------------------------------------
-struct Lll {
-    int64_t *B;
-    i128 *G;
-    double *mu, *bb;
+template <int N> struct Lll {
+    LllMem<N> *S;
     int n, M;
 };
 
-// b_k -= q b_j, on the vectors and the exact Gram; true on overflow
-__device__ bool lll_sub(Lll &L, int k, int j, int64_t q, int lane)
+// mu(k, j) (j < k) and bb[k] from G(k, .) and the rows above: r_j = mu_kj
+// bb_j solves the unit lower-triangular system r_j = G_kj - sum_{l<j} mu_jl
+// r_l (forward substitution by columns, lanes own rows).
+template <int N> PFG_NOINLINE __device__ void lll_gs(LllMem<N> *S, int k, int lane)
 {
-    bool bad = false;
-    for (int c = lane; c < L.n; c += 32) {
-        i128 x = (i128)L.B[k * MH + c] - (i128)q * L.B[j * MH + c];
-        if (!fits64(x)) bad = true;
-        else L.B[k * MH + c] = (int64_t)x;
-    }
-    i128 gkk = 0;
-    {
-        i128 t, u;
-        bool b = mul_ovf(L.G[j * LDG + j], (i128)q, &t) ||
-                 sub_ovf(t, L.G[k * LDG + j], &t) || sub_ovf(t, L.G[k * LDG + j], &t) ||
-                 mul_ovf(t, (i128)q, &u) || add_ovf(L.G[k * LDG + k], u, &gkk);
-        bad |= b;
-    }
-    __syncwarp();
-    for (int l = lane; l < L.M; l += 32) {
-        if (l == k) continue;
-        i128 t;
-        if (mul_ovf(L.G[j * LDG + l], (i128)q, &t) || sub_ovf(L.G[k * LDG + l], t, &t)) { bad = true; continue; }
-        L.G[k * LDG + l] = t;
-        L.G[l * LDG + k] = t;
-    }
-    __syncwarp();
-    if (lane == 0) L.G[k * LDG + k] = gkk;
-    __syncwarp();
-    return warp_any(bad);
-}
-
-// Gram-Schmidt data of row k from the exact Gram: r_j = mu_kj bb_j solves
-// the unit lower-triangular system r_j = G_kj - sum_{l<j} mu_jl r_l
-// (column-oriented forward substitution, lanes own rows).
-__device__ void lll_gs(Lll &L, int k, int lane)
-{
-    double a0 = lane < k ? (double)L.G[k * LDG + lane] : 0.0;
-    double a1 = lane + 32 < k ? (double)L.G[k * LDG + lane + 32] : 0.0;
+    double a0 = lane < k ? (double)S->G[gix(k, lane)] : 0.0;
+    double a1 = 0.0;
+    if (N > 32) a1 = lane + 32 < k ? (double)S->G[gix(k, lane + 32)] : 0.0;
     double s = 0.0;
+    double *muk = S->mu + mix(k, 0);
     for (int j = 0; j < k; ++j) {
-        double rj = __shfl_sync(FULL, j < 32 ? a0 : a1, j & 31);
-        double mkj = rj / L.bb[j];
-        if (lane == (j & 31)) L.mu[k * MH + j] = mkj;
-        s += mkj * rj;
-        if (lane > j && lane < k) a0 -= L.mu[lane * MH + j] * rj;
-        if (lane + 32 > j && lane + 32 < k) a1 -= L.mu[(lane + 32) * MH + j] * rj;
+        const double rj = __shfl_sync(FULL, (N > 32 && j >= 32) ? a1 : a0, j & 31);
+        const double mkj = rj * S->ibb[j];
+        s = fma(mkj, rj, s);
+        if (lane == (j & 31)) muk[j] = mkj;
+        if (lane > j && lane < k) a0 = fma(-S->mu[mix(lane, j)], rj, a0);
+        if (N > 32 && lane + 32 > j && lane + 32 < k) a1 = fma(-S->mu[mix(lane + 32, j)], rj, a1);
     }
-    if (lane == 0) L.bb[k] = (double)L.G[k * LDG + k] - s;
-    __syncwarp();
-}
-
-__device__ void lll_swap(Lll &L, int k, int lane)
-{
-    for (int c = lane; c < L.n; c += 32) {
-        int64_t t = L.B[k * MH + c]; L.B[k * MH + c] = L.B[(k - 1) * MH + c]; L.B[(k - 1) * MH + c] = t;
-    }
-    __syncwarp();
-    for (int l = lane; l < L.M; l += 32) {
-        i128 t = L.G[k * LDG + l]; L.G[k * LDG + l] = L.G[(k - 1) * LDG + l]; L.G[(k - 1) * LDG + l] = t;
-    }
-    __syncwarp();
-    for (int l = lane; l < L.M; l += 32) {
-        i128 t = L.G[l * LDG + k]; L.G[l * LDG + k] = L.G[l * LDG + k - 1]; L.G[l * LDG + k - 1] = t;
+    if (lane == 0) {
+        const double b = (double)S->G[gix(k, k)] - s;
+        S->bb[k] = b;
+        S->ibb[k] = 1.0 / b;
     }
     __syncwarp();
 }
 
-__device__ int warp_lll(Lll &L, int m, bool has_last, int lane)
+// Size-reduce row k against rows 0..k-1: the multipliers q_j come from the
+// Gram-Schmidt row (Babai), then b_k -= sum_j q_j b_j in one exact pass over
+// B and G; repeated until no multiplier is non-zero.  Leaves row k's
+// Gram-Schmidt data current.
+template <int N> PFG_NOINLINE __device__ int lll_reduce(Lll<N> &L, int k, int lane)
 {
-    const double delta = 0.99;
-    L.M = m + (has_last ? 1 : 0);
-    if (m >= 1) {
-        lll_gs(L, 0, lane);
-        if (!(L.bb[0] > 0)) return ST_OVERFLOW;
-    }
-    if (m >= 2) lll_gs(L, 1, lane);
-    int k = 1, iters = 0;
-    while (k < m) {
-        if (++iters > 200000) return ST_OVERFLOW;
-        for (int pass = 0; pass < 4; ++pass) {
-            bool changed = false;
-            for (int j = k - 1; j >= 0; --j) {
-                double q = rint(L.mu[k * MH + j]);
-                if (q == 0.0) continue;
-                if (!(fabs(q) <= 9.0e18)) return ST_OVERFLOW;
-                int64_t qi = (int64_t)q;
-                if (lll_sub(L, k, j, qi, lane)) return ST_OVERFLOW;
-                for (int l = lane; l < j; l += 32) L.mu[k * MH + l] -= q * L.mu[j * MH + l];
-                __syncwarp();
-                if (lane == 0) L.mu[k * MH + j] -= q;
-                __syncwarp();
-                changed = true;
-            }
-            if (!changed) break;
-            lll_gs(L, k, lane);
+    LllMem<N> *S = L.S;
+    for (int pass = 0; pass < 16; ++pass) {
+        double r0 = lane < k ? S->mu[mix(k, lane)] : 0.0;
+        double r1 = 0.0;
+        if (N > 32) r1 = lane + 32 < k ? S->mu[mix(k, lane + 32)] : 0.0;
+        bool any = false;
+        for (int j = k - 1; j >= 0; --j) {
+            const double x = __shfl_sync(FULL, (N > 32 && j >= 32) ? r1 : r0, j & 31);
+            const double qd = rint(x);
+            PFG_UNIFORM(qd);
+            if (!(fabs(qd) <= 9.0e18)) return ST_OVERFLOW;
+            if (lane == 0) S->q[j] = (int64_t)qd;
+            if (qd == 0.0) continue;
+            any = true;
+            if (lane < j) r0 = fma(-qd, S->mu[mix(j, lane)], r0);
+            if (N > 32 && lane + 32 < j) r1 = fma(-qd, S->mu[mix(j, lane + 32)], r1);
         }
-        if (!(L.bb[k] > 0)) return ST_OVERFLOW;
-        double mk = L.mu[k * MH + k - 1];
-        if (L.bb[k] < (delta - mk * mk) * L.bb[k - 1]) {
-            lll_swap(L, k, lane);
-            k = k > 1 ? k - 1 : 1;
-            if (k == 1) lll_gs(L, 0, lane);
-            lll_gs(L, k - 1, lane);
-            lll_gs(L, k, lane);
-        } else {
-            ++k;
-            if (k < m) lll_gs(L, k, lane);
-        }
-    }
-    if (has_last && m > 0) {            // size-reduce row m against rows 0..m-1
-        double *mw = L.mu + m * MH;     // (row m of mu is free: m <= MD - 1)
-        for (int pass = 0; pass < 4; ++pass) {
-            // mw_j bb_j = G_mj - sum_{l<j} mu_jl mw_l bb_l  (forward substitution)
-            double a0 = lane < m ? (double)L.G[m * LDG + lane] : 0.0;
-            double a1 = lane + 32 < m ? (double)L.G[m * LDG + lane + 32] : 0.0;
-            for (int j = 0; j < m; ++j) {
-                double rj = __shfl_sync(FULL, j < 32 ? a0 : a1, j & 31);
-                if (lane == (j & 31)) mw[j] = rj / L.bb[j];
-                if (lane > j && lane < m) a0 -= L.mu[lane * MH + j] * rj;
-                if (lane + 32 > j && lane + 32 < m) a1 -= L.mu[(lane + 32) * MH + j] * rj;
+        if (!any) return 0;
+        PFG_COUNT(2, 1);
+        __syncwarp();                                   // q[] visible to all lanes
+        bool bad = false;
+        // new row k of B (lanes own columns)
+        i128 b0 = 0, b1 = 0;
+        if (lane < L.n) {
+            b0 = S->B[k * N + lane];
+            for (int j = 0; j < k; ++j) {
+                const int64_t qj = S->q[j];
+                if (qj) bad |= submul_ovf(b0, qj, (i128)S->B[j * N + lane]);
             }
-            __syncwarp();
-            bool changed = false;
-            for (int j = m - 1; j >= 0; --j) {
-                double q = rint(mw[j]);
-                if (q == 0.0) continue;
-                if (!(fabs(q) <= 9.0e18)) return ST_OVERFLOW;
-                if (lll_sub(L, m, j, (int64_t)q, lane)) return ST_OVERFLOW;
-                for (int l = lane; l < j; l += 32) mw[l] -= q * L.mu[j * MH + l];
-                __syncwarp();
-                if (lane == 0) mw[j] -= q;
-                __syncwarp();
-                changed = true;
-            }
-            if (!changed) break;
         }
+        if (N > 32 && lane + 32 < L.n) {
+            b1 = S->B[k * N + lane + 32];
+            for (int j = 0; j < k; ++j) {
+                const int64_t qj = S->q[j];
+                if (qj) bad |= submul_ovf(b1, qj, (i128)S->B[j * N + lane + 32]);
+            }
+        }
+        bad |= !fits64(b0) || !fits64(b1);
+        // new G(k, l), l != k (lanes own l)
+        const int l0 = lane, l1 = lane + 32;
+        i128 g0 = 0, g1 = 0;
+        if (l0 < L.M && l0 != k) {
+            g0 = S->G[gix(k, l0)];
+            for (int j = 0; j < k; ++j) {
+                const int64_t qj = S->q[j];
+                if (qj) bad |= submul_ovf(g0, qj, S->G[gix(j, l0)]);
+            }
+        }
+        if (N > 32 && l1 < L.M && l1 != k) {
+            g1 = S->G[gix(k, l1)];
+            for (int j = 0; j < k; ++j) {
+                const int64_t qj = S->q[j];
+                if (qj) bad |= submul_ovf(g1, qj, S->G[gix(j, l1)]);
+            }
+        }
+        // G'(k, k) = G(k, k) - sum_{l<k} q_l (G(k, l) + G'(k, l))
+        i128 t = 0;
+        if (l0 < k && S->q[l0]) {
+            i128 u, v;
+            bad |= add_ovf(S->G[gix(k, l0)], g0, &u);
+            bad |= mul_ovf((i128)S->q[l0], u, &v);
+            t = v;
+        }
+        if (N > 32 && l1 < k && S->q[l1]) {
+            i128 u, v;
+            bad |= add_ovf(S->G[gix(k, l1)], g1, &u);
+            bad |= mul_ovf((i128)S->q[l1], u, &v);
+            bad |= add_ovf(t, v, &t);
+        }
+        for (int o = 16; o; o >>= 1) bad |= add_ovf(t, shfl_xor_i128(t, o), &t);
+        i128 gkk;
+        bad |= sub_ovf(S->G[gix(k, k)], t, &gkk);
+        if (warp_any(bad)) return ST_OVERFLOW;
+        __syncwarp();                                   // every lane has read the old row k
+        if (lane < L.n) S->B[k * N + lane] = (int64_t)b0;
+        if (N > 32 && lane + 32 < L.n) S->B[k * N + lane + 32] = (int64_t)b1;
+        if (l0 < L.M && l0 != k) S->G[gix(k, l0)] = g0;
+        if (N > 32 && l1 < L.M && l1 != k) S->G[gix(k, l1)] = g1;
+        if (lane == 0) S->G[gix(k, k)] = gkk;
+        __syncwarp();
+        lll_gs(S, k, lane);
     }
     return 0;
 }
 
-// Euclidean Gram of rows 0..m-1 of B (length n)
-__device__ bool gram_euclid(SetupScratch *W, int m, int n, int lane)
+// Exchange rows k-1 and k: B, G exactly; the Gram-Schmidt data of the two
+// rows by the usual update formulas (rows > k are recomputed when visited).
+template <int N> PFG_NOINLINE __device__ void lll_swap(Lll<N> &L, int k, int lane)
+{
+    LllMem<N> *S = L.S;
+    for (int c = lane; c < L.n; c += 32) {
+        const int64_t t = S->B[k * N + c];
+        S->B[k * N + c] = S->B[(k - 1) * N + c];
+        S->B[(k - 1) * N + c] = t;
+    }
+    for (int l = lane; l < L.M; l += 32) {
+        if (l == k || l == k - 1) continue;
+        const i128 t = S->G[gix(k, l)];
+        S->G[gix(k, l)] = S->G[gix(k - 1, l)];
+        S->G[gix(k - 1, l)] = t;
+    }
+    for (int j = lane; j < k - 1; j += 32) {
+        const double t = S->mu[mix(k, j)];
+        S->mu[mix(k, j)] = S->mu[mix(k - 1, j)];
+        S->mu[mix(k - 1, j)] = t;
+    }
+    if (lane == 0) {
+        const i128 t = S->G[gix(k, k)];
+        S->G[gix(k, k)] = S->G[gix(k - 1, k - 1)];
+        S->G[gix(k - 1, k - 1)] = t;
+        const double m = S->mu[mix(k, k - 1)], b1 = S->bb[k - 1], b2 = S->bb[k];
+        const double Bn = k == 1 ? (double)S->G[0] : fma(m * m, b1, b2);
+        S->mu[mix(k, k - 1)] = m * b1 / Bn;
+        S->bb[k] = b1 * b2 / Bn;
+        S->bb[k - 1] = Bn;
+        S->ibb[k] = 1.0 / S->bb[k];
+        S->ibb[k - 1] = 1.0 / Bn;
+    }
+    __syncwarp();
+}
+
+template <int N> PFG_NOINLINE __device__ int warp_lll(Lll<N> &L, int m, bool has_last, double delta, int lane)
+{
+    LllMem<N> *S = L.S;
+    L.M = m + (has_last ? 1 : 0);
+    PFG_COUNT(0, 1);
+    if (m >= 1) {
+        lll_gs(S, 0, lane);
+        if (!(S->bb[0] > 0)) return ST_OVERFLOW;
+    }
+    if (m >= 2) lll_gs(S, 1, lane);
+    int k = 1, iters = 0;
+    while (k < m) {
+        if (++iters > 200000) return ST_OVERFLOW;
+        int st = lll_reduce(L, k, lane);
+        if (st) return st;
+        const double bk = S->bb[k], mk = S->mu[mix(k, k - 1)], bk1 = S->bb[k - 1];
+        PFG_UNIFORM(bk);
+        __syncwarp();                       // (every lane has read them before lll_swap writes)
+        if (!(bk > 0)) return ST_OVERFLOW;
+        if (bk < (delta - mk * mk) * bk1) {
+            lll_swap(L, k, lane);
+            PFG_COUNT(1, 1);
+            if (k > 1) --k;
+        } else {
+            ++k;
+            if (k < m) lll_gs(S, k, lane);
+        }
+    }
+    if (has_last && m > 0) {
+        lll_gs(S, m, lane);
+        int st = lll_reduce(L, m, lane);
+        if (st) return st;
+    }
+    return 0;
+}
+
+// Euclidean Gram of rows 0..m-1 of B (length n); true on overflow
+template <int N> PFG_NOINLINE __device__ bool gram_euclid(LllMem<N> *S, int m, int n, int lane)
 {
     bool bad = false;
-    for (int e = lane; e < m * m; e += 32) {
-        int i = e / m, j = e % m;
-        if (j > i) continue;
+    for (int e = lane; e < (m * (m + 1)) / 2; e += 32) {
+        int i, j;
+        tri_of(e, i, j);
         i128 s = 0;
         for (int c = 0; c < n; ++c)
-            if (add_ovf(s, (i128)W->B[i * MH + c] * W->B[j * MH + c], &s)) bad = true;
-        W->G[i * LDG + j] = s;
-        W->G[j * LDG + i] = s;
+            if (add_ovf(s, (i128)S->B[i * N + c] * S->B[j * N + c], &s)) bad = true;
+        S->G[e] = s;
     }
     __syncwarp();
     return warp_any(bad);
+}
+
+// Exchange rows a and b (any positions) of B and G; Gram-Schmidt data become stale.
+template <int N> PFG_NOINLINE __device__ void lll_exchange(Lll<N> &L, int a, int b, int lane)
+{
+    if (a == b) return;
+    LllMem<N> *S = L.S;
+    for (int c = lane; c < L.n; c += 32) {
+        const int64_t t = S->B[a * N + c];
+        S->B[a * N + c] = S->B[b * N + c];
+        S->B[b * N + c] = t;
+    }
+    for (int l = lane; l < L.M; l += 32) {
+        if (l == a || l == b) continue;
+        const i128 t = S->G[gix(a, l)];
+        S->G[gix(a, l)] = S->G[gix(b, l)];
+        S->G[gix(b, l)] = t;
+    }
+    if (lane == 0) {
+        const i128 t = S->G[gix(a, a)];
+        S->G[gix(a, a)] = S->G[gix(b, b)];
+        S->G[gix(b, b)] = t;
+    }
+    __syncwarp();
+}
+
+// One elimination step of column col over rows 0..nr-1 with pivot row pr:
+// b_r -= floor(b_r[col] / b_pr[col]) b_pr for every r != pr, exactly, with
+// the Gram updated as E G E^T.  True on overflow.
+template <int N> PFG_NOINLINE __device__ bool echelon_step(Lll<N> &L, int nr, int pr, int col, int lane)
+{
+    LllMem<N> *S = L.S;
+    const int64_t piv = S->B[pr * N + col];
+    for (int r = lane; r < nr; r += 32) S->q[r] = r == pr ? 0 : fdiv64(S->B[r * N + col], piv);
+    for (int l = lane; l < nr; l += 32) S->T[l] = S->G[gix(pr, l)];
+    __syncwarp();
+    bool bad = false;
+    for (int c = lane; c < L.n; c += 32) {
+        const int64_t bp = S->B[pr * N + c];
+        for (int r = 0; r < nr; ++r) {
+            const int64_t qr = S->q[r];
+            if (!qr) continue;
+            const i128 x = (i128)S->B[r * N + c] - (i128)qr * bp;
+            if (!fits64(x)) { bad = true; continue; }
+            S->B[r * N + c] = (int64_t)x;
+        }
+    }
+    const i128 tp = S->T[pr];
+    for (int e = lane; e < (nr * (nr + 1)) / 2; e += 32) {
+        int r, l;
+        tri_of(e, r, l);
+        const int64_t qr = S->q[r], ql = S->q[l];
+        if (!qr && !ql) continue;
+        i128 g;
+        if (r == pr || l == pr) {                      // <b_o - q_o b_pr, b_pr>
+            const int o = r == pr ? l : r;
+            g = S->T[o];
+            bad |= submul_ovf(g, S->q[o], tp);
+        } else {                                       // G - q_r T_l - q_l T_r + q_r q_l T_pr
+            g = S->G[e];
+            bad |= submul_ovf(g, qr, S->T[l]);
+            bad |= submul_ovf(g, ql, S->T[r]);
+            i128 qq = (i128)qr * ql, t;
+            if (mul_ovf(qq, tp, &t) || add_ovf(g, t, &g)) bad = true;
+        }
+        S->G[e] = g;
+    }
+    __syncwarp();
+    return warp_any(bad);
+}
+
+// warp argmin over rows r < nr of |B[r][col]| != 0 (-1 if the column is 0)
+template <int N> PFG_NOINLINE __device__ int argmin_nonzero(const int64_t *B, int nr, int col, int lane)
+{
+    uint64_t best = ~0ull;
+    int who = -1;
+    for (int r = lane; r < nr; r += 32) {
+        uint64_t a = uabs64(B[r * N + col]);
+        if (a && a < best) { best = a; who = r; }
+    }
+    for (int o = 16; o; o >>= 1) {
+        uint64_t ob = __shfl_xor_sync(FULL, best, o);
+        int ow = __shfl_xor_sync(FULL, who, o);
+        if (ob < best || (ob == best && ow >= 0 && (who < 0 || ow < who))) { best = ob; who = ow; }
+    }
+    return who;
 }
 
 // Unimodular U (n x n rows, stride MH, into Uo) with U v = (gcd, 0, ..., 0)
@@ -242,7 +459,7 @@ __device__ bool gram_euclid(SetupScratch *W, int m, int n, int lane)
 // running gcd is then 1, every later step is (1, w_k) -> (1, 0), and the
 // entries stay below about max|v|^2 instead of compounding.  Any unimodular
 // U gives the same lattice; v is read from vin (length n).
-__device__ int warp_unimodular(const int64_t *vin, int n, int64_t *Uo, int64_t *wtmp, int *perm, int lane)
+PFG_NOINLINE __device__ int warp_unimodular(const int64_t *vin, int n, int64_t *Uo, int64_t *wtmp, int *perm, int lane)
 {
     // g = gcd(v)
     uint64_t g = 0;
@@ -310,27 +527,14 @@ __device__ int warp_unimodular(const int64_t *vin, int n, int64_t *Uo, int64_t *
     return 0;
 }
 
-// warp argmin over rows r < nr of |B[r][col]| != 0 (-1 if the column is 0)
-__device__ int argmin_nonzero(const int64_t *B, int nr, int col, int lane)
-{
-    uint64_t best = ~0ull;
-    int who = -1;
-    for (int r = lane; r < nr; r += 32) {
-        uint64_t a = uabs64(B[r * MH + col]);
-        if (a && a < best) { best = a; who = r; }
-    }
-    for (int o = 16; o; o >>= 1) {
-        uint64_t ob = __shfl_xor_sync(FULL, best, o);
-        int ow = __shfl_xor_sync(FULL, who, o);
-        if (ob < best || (ob == best && ow >= 0 && (who < 0 || ow < who))) { best = ob; who = ow; }
-    }
-    return who;
-}
+#ifndef PFG_DELTA_H
+#define PFG_DELTA_H 0.99
+#endif
 
 // ---------------------------------------------------------------------------
-// The setup of one direction.
+// The setup of one direction; S is the warp's LLL working set (N >= h11).
 // ---------------------------------------------------------------------------
-__device__ int setup_one(const SetupArgs &A, int pid, int lane, int &stage)
+template <int N> __device__ int setup_one(const SetupArgs &A, int pid, int lane, int &stage, LllMem<N> *S)
 {
     SetupScratch *W = A.scratch + (blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5));
     const Geo g = A.geo[A.pgeo[pid]];
@@ -340,8 +544,9 @@ __device__ int setup_one(const SetupArgs &A, int pid, int lane, int &stage)
     const Slab L = slab_layout(h, d);
     Dir &D = A.dirs[pid];
     bool bad = false;
+    StageClock clk(stage, lane);
 
-    stage = 1;
+    clk.mark(1);
     // 1. Z = kappa . p
     for (int e = lane; e < h * h; e += 32) {
         i128 s = 0;
@@ -352,7 +557,7 @@ __device__ int setup_one(const SetupArgs &A, int pid, int lane, int &stage)
     }
     __syncwarp();
     if (warp_any(bad)) return ST_OVERFLOW;
-    stage = 2;
+    clk.mark(2);
     // 2. T = Z p, v = T Mbasis
     for (int i = lane; i < h; i += 32) {
         i128 s = 0;
@@ -372,24 +577,26 @@ __device__ int setup_one(const SetupArgs &A, int pid, int lane, int &stage)
     }
     __syncwarp();
     if (warp_any(bad)) return ST_OVERFLOW;
-    stage = 3;
+    clk.mark(3);
     // 3. orthogonal lattice: rows 1.. of the unimodular transform of v
     int st = warp_unimodular(W->v, h, W->V, W->w, W->order, lane);
     if (st) return st;
-    for (int e = lane; e < d * h; e += 32) W->B[(e / h) * MH + e % h] = W->V[(e / h + 1) * MH + e % h];
+    for (int e = lane; e < d * h; e += 32) S->B[(e / h) * N + e % h] = W->V[(e / h + 1) * MH + e % h];
     __syncwarp();
-    stage = 4;
+    clk.mark(4);
     // 4. Euclidean LLL of O
-    if (gram_euclid(W, d, h, lane)) return ST_OVERFLOW;
-    Lll LL{W->B, W->G, W->mu, W->bb, h, d};
-    if ((st = warp_lll(LL, d, false, lane))) return st;
-    stage = 5;
+    if (gram_euclid<N>(S, d, h, lane)) return ST_OVERFLOW;
+    {
+        Lll<N> LL{S, h, d};
+        if ((st = warp_lll(LL, d, false, 0.99, lane))) return st;
+    }
+    clk.mark(5);
     // 5. (Mbasis O^T)^T rows, 6. coni order (rows with entry 0 == 0 first, stable)
     for (int e = lane; e < d * h; e += 32) {
         int a = e / h, i = e % h;
         i128 s = 0;
         for (int l = 0; l < h; ++l)
-            if (add_ovf(s, (i128)Mb[i * h + l] * W->B[a * MH + l], &s)) bad = true;
+            if (add_ovf(s, (i128)Mb[i * h + l] * S->B[a * N + l], &s)) bad = true;
         if (!fits64(s)) bad = true;
         W->S[a * MH + i] = (int64_t)s;
     }
@@ -404,7 +611,7 @@ __device__ int setup_one(const SetupArgs &A, int pid, int lane, int &stage)
     int64_t *BT = slab + L.bt, *ZT = slab + L.zt, *MAT = slab + L.mat;
     for (int e = lane; e < d * h; e += 32) BT[e] = W->S[W->order[e / h] * MH + e % h];
     __syncwarp();
-    stage = 7;
+    clk.mark(7);
     // 7. ZT[a][r] = (Z Binter)[r][a], mat = -Binter^T Z Binter
     for (int e = lane; e < d * h; e += 32) {
         int a = e / h, r = e % h;
@@ -427,7 +634,7 @@ __device__ int setup_one(const SetupArgs &A, int pid, int lane, int &stage)
     __syncwarp();
     if (warp_any(bad)) return ST_OVERFLOW;
 
-    stage = 8;
+    clk.mark(8);
     // 8. cut-aware basis (pfv_lattice.h:554-602)
     for (int a = lane; a < d; a += 32) W->v[a] = BT[a * h];
     __syncwarp();
@@ -441,39 +648,40 @@ __device__ int setup_one(const SetupArgs &A, int pid, int lane, int &stage)
         // B rows 0..d-2 = K = V[1..], row d-1 = w = V[0]
         for (int e = lane; e < d * d; e += 32) {
             int a = e / d, c = e % d;
-            W->B[a * MH + c] = a < d - 1 ? W->V[(a + 1) * MH + c] : W->V[c];
+            S->B[a * N + c] = a < d - 1 ? W->V[(a + 1) * MH + c] : W->V[c];
         }
         __syncwarp();
-        // Gram w.r.t. mat: G_ij = B_i^T mat B_j
+        // Gram w.r.t. mat: G_ij = B_i^T mat B_j  (T holds mat B_j)
         for (int j = 0; j < d; ++j) {
             for (int c = lane; c < d; c += 32) {
                 i128 s = 0;
                 for (int k = 0; k < d; ++k)
-                    if (add_ovf(s, (i128)MAT[c * d + k] * W->B[j * MH + k], &s)) bad = true;
-                W->y[c] = s;
+                    if (add_ovf(s, (i128)MAT[c * d + k] * S->B[j * N + k], &s)) bad = true;
+                S->T[c] = s;
             }
             __syncwarp();
             for (int i = lane; i <= j; i += 32) {
                 i128 s = 0, t;
                 for (int c = 0; c < d; ++c) {
-                    if (!W->B[i * MH + c]) continue;
-                    if (mul_ovf(W->y[c], (i128)W->B[i * MH + c], &t) || add_ovf(s, t, &s)) bad = true;
+                    if (!S->B[i * N + c]) continue;
+                    if (mul_ovf(S->T[c], (i128)S->B[i * N + c], &t) || add_ovf(s, t, &s)) bad = true;
                 }
-                W->G[i * LDG + j] = s;
-                W->G[j * LDG + i] = s;
+                S->G[gix(j, i)] = s;
             }
             __syncwarp();
         }
         if (warp_any(bad)) return ST_OVERFLOW;
-        Lll LK{W->B, W->G, W->mu, W->bb, d, d};
-        if ((st = warp_lll(LK, d - 1, true, lane))) return st;
+        {
+            Lll<N> LK{S, d, d};
+            if ((st = warp_lll(LK, d - 1, true, 0.99, lane))) return st;
+        }
         // new columns a of Binter: sum_b B[a][b] Binter[:, b]  (likewise ZB)
         for (int e = lane; e < d * h; e += 32) {
             int a = e / h, r = e % h;
             i128 s = 0, t = 0;
             for (int b = 0; b < d; ++b) {
-                s += (i128)W->B[a * MH + b] * BT[b * h + r];
-                t += (i128)W->B[a * MH + b] * ZT[b * h + r];
+                s += (i128)S->B[a * N + b] * BT[b * h + r];
+                t += (i128)S->B[a * N + b] * ZT[b * h + r];
             }
             if (!fits64(s) || !fits64(t)) bad = true;
             W->S[a * MH + r] = (int64_t)s;
@@ -486,7 +694,7 @@ __device__ int setup_one(const SetupArgs &A, int pid, int lane, int &stage)
             ZT[e] = W->V[(e / h) * MH + e % h];
         }
         for (int e = lane; e < d * d; e += 32) {
-            i128 x = W->G[(e / d) * LDG + e % d];
+            i128 x = S->G[gix(e / d, e % d)];
             if (!fits64(x)) bad = true;
             MAT[e] = (int64_t)x;
         }
@@ -501,12 +709,14 @@ __device__ int setup_one(const SetupArgs &A, int pid, int lane, int &stage)
         return ST_EMPTY;
     }
 
-    stage = 9;
+    clk.mark(9);
     // 9. GCD rows: echelon basis of the row lattice of ZB[1:] with small rows.
     // The rows r_k = ZB[k][:], k = 1..d, satisfy sum_k p_k r_k = 0 (p^T Z Binter
     // = 0 and p_0 = 0); with V p' = e0 from Bezout steps, the rows of V^-T R
     // are the rows of R with row 0 = p'^T R = 0: drop it, the rest is a basis.
-    for (int e = lane; e < d * d; e += 32) W->B[(e / d) * MH + e % d] = ZT[(e % d) * h + e / d + 1];
+    // (Lanes own columns here, so the row operations need no staging.)
+    for (int c = lane; c < d; c += 32)
+        for (int r = 0; r < d; ++r) S->B[r * N + c] = ZT[c * h + r + 1];
     for (int e = lane; e < d; e += 32) W->w[e] = p[e + 1];
     __syncwarp();
     for (int k = 1; k < d; ++k) {
@@ -518,90 +728,75 @@ __device__ int setup_one(const SetupArgs &A, int pid, int lane, int &stage)
         __syncwarp();
         if (lane == 0) { W->w[0] = gg; W->w[k] = 0; }
         for (int c = lane; c < d; c += 32) {
-            i128 r0 = (i128)m11 * W->B[c] - (i128)m10 * W->B[k * MH + c];
-            i128 rk = -(i128)t * W->B[c] + (i128)s * W->B[k * MH + c];
+            i128 r0 = (i128)m11 * S->B[c] - (i128)m10 * S->B[k * N + c];
+            i128 rk = -(i128)t * S->B[c] + (i128)s * S->B[k * N + c];
             if (!fits64(r0) || !fits64(rk)) { bad = true; continue; }
-            W->B[c] = (int64_t)r0;
-            W->B[k * MH + c] = (int64_t)rk;
+            S->B[c] = (int64_t)r0;
+            S->B[k * N + c] = (int64_t)rk;
         }
         __syncwarp();
         if (warp_any(bad)) return ST_OVERFLOW;
     }
-    stage = 91;
-    for (int c = lane; c < d; c += 32) bad |= W->B[c] != 0;
+    clk.mark(91);
+    for (int c = lane; c < d; c += 32) bad |= S->B[c] != 0;
     if (warp_any(bad)) return ST_OVERFLOW;          // p'^T ZB[1:] must vanish exactly
-    int nr = d - 1;
-    // drop row 0 (staged through S: an in-place shift would race across lanes)
-    for (int e = lane; e < nr * d; e += 32) W->S[(e / d) * MH + e % d] = W->B[(e / d + 1) * MH + e % d];
-    __syncwarp();
-    for (int e = lane; e < nr * d; e += 32) W->B[(e / d) * MH + e % d] = W->S[(e / d) * MH + e % d];
-    __syncwarp();
     int64_t *H = slab + L.H;
     for (int e = lane; e < d * d; e += 32) H[e] = 0;
     uint64_t hrows = 0;
-    if (nr > 0) {
+    {
+        int nr = d - 1;
+        for (int c = lane; c < d; c += 32)          // drop row 0
+            for (int r = 0; r < nr; ++r) S->B[r * N + c] = S->B[(r + 1) * N + c];
+        __syncwarp();
         // Rows whose construction would leave int64 (the last pivots are
         // large: the lattice of rows vanishing on all but the last columns has
         // a huge covolume) are not built: the rows found so far are kept, and
         // any set of rows of the lattice gives a valid GCD bound.
-        if (gram_euclid(W, nr, d, lane)) goto h_done;
-        Lll LH{W->B, W->G, W->mu, W->bb, d, nr};
-        if (warp_lll(LH, nr, false, lane)) goto h_done;
-        for (int col = 0; col < d && nr > 0; ++col) {
-            int pr = -1;
-            for (int it = 0; ; ++it) {
-                if (it > 256) goto h_done;
-                pr = argmin_nonzero(W->B, nr, col, lane);
-                PFG_UNIFORM(pr);
-                if (pr < 0) break;
-                bool other = false;
+        if (nr > 0) {
+            if (gram_euclid<N>(S, nr, d, lane)) goto h_done;
+            Lll<N> LH{S, d, nr};
+            if (warp_lll(LH, nr, false, PFG_DELTA_H, lane)) goto h_done;
+            for (int col = 0; col < d && nr > 0; ++col) {
+                int pr = -1;
                 LH.M = nr;
-                for (int r = 0; r < nr; ++r) {
-                    if (r == pr) continue;
-                    int64_t x = W->B[r * MH + col];
-                    PFG_UNIFORM(x);
-                    if (!x) continue;
-                    int64_t q = fdiv64(x, W->B[pr * MH + col]);
-                    PFG_UNIFORM(q);
-                    __syncwarp();           // (every lane has read row r before lll_sub writes it)
-                    if (lll_sub(LH, r, pr, q, lane)) goto h_done;
-                    other |= W->B[r * MH + col] != 0;
+                for (int it = 0; ; ++it) {
+                    if (it > 256) goto h_done;
+                    pr = argmin_nonzero<N>(S->B, nr, col, lane);
+                    PFG_UNIFORM(pr);
+                    if (pr < 0) break;
+                    bool other = false;
+                    for (int r = lane; r < nr; r += 32) other |= r != pr && S->B[r * N + col] != 0;
+                    if (!warp_any(other)) break;
+                    if (echelon_step(LH, nr, pr, col, lane)) goto h_done;
                 }
-                PFG_UNIFORM(other);
-                if (!other) break;
-            }
-            if (pr < 0) continue;
-            // move the pivot row to the end (index nr - 1), positive pivot
-            LH.M = nr;
-            for (int k2 = pr + 1; k2 < nr; ++k2) lll_swap(LH, k2, lane);
-            const bool neg = W->B[(nr - 1) * MH + col] < 0;
-            PFG_UNIFORM(neg);
-            __syncwarp();                   // (read by every lane before the owner negates it)
-            if (neg) {
-                for (int c = lane; c < d; c += 32) W->B[(nr - 1) * MH + c] = -W->B[(nr - 1) * MH + c];
-                for (int l = lane; l < nr; l += 32) {
-                    if (l == nr - 1) continue;
-                    W->G[(nr - 1) * LDG + l] = -W->G[(nr - 1) * LDG + l];
-                    W->G[l * LDG + nr - 1] = -W->G[l * LDG + nr - 1];
+                if (pr < 0) continue;
+                // the pivot row to the end (index nr - 1), positive pivot
+                lll_exchange(LH, pr, nr - 1, lane);
+                const bool neg = S->B[(nr - 1) * N + col] < 0;
+                PFG_UNIFORM(neg);
+                __syncwarp();                   // (read by every lane before the owner negates it)
+                if (neg) {
+                    for (int c = lane; c < d; c += 32) S->B[(nr - 1) * N + c] = -S->B[(nr - 1) * N + c];
+                    for (int l = lane; l < nr - 1; l += 32) S->G[gix(nr - 1, l)] = -S->G[gix(nr - 1, l)];
+                    __syncwarp();
+                }
+                // LLL the rows below (rows 0..nr-2), size-reduce the pivot row against them
+                if (warp_lll(LH, nr - 1, true, PFG_DELTA_H, lane)) goto h_done;
+                bool fits = true;
+                for (int c = lane; c < d; c += 32) fits &= uabs64(S->B[(nr - 1) * N + c]) < (1ull << 62);
+                fits = __all_sync(FULL, fits);
+                if (fits) {
+                    for (int c = lane; c < d; c += 32) H[col * d + c] = S->B[(nr - 1) * N + c];
+                    hrows |= 1ull << col;
                 }
                 __syncwarp();
+                --nr;
             }
-            // LLL the rows below (rows 0..nr-2), size-reduce the pivot row against them
-            if (warp_lll(LH, nr - 1, true, lane)) goto h_done;
-            bool fits = true;
-            for (int c = lane; c < d; c += 32) fits &= uabs64(W->B[(nr - 1) * MH + c]) < (1ull << 62);
-            fits = __all_sync(FULL, fits);
-            if (fits) {
-                for (int c = lane; c < d; c += 32) H[col * d + c] = W->B[(nr - 1) * MH + c];
-                hrows |= 1ull << col;
-            }
-            __syncwarp();
-            --nr;
         }
     }
 h_done:
 
-    stage = 10;
+    clk.mark(10);
     // 10. FP64 Cholesky of mat, certificate, float copies
     double *U = (double *)(slab + L.u64);
     for (int e = lane; e < d * d; e += 32) U[e] = 0.0;
@@ -657,7 +852,7 @@ h_done:
     for (int e = lane; e < d * d; e += 32) U32[e] = (float)U[e];
     __syncwarp();
     for (int i = lane; i < d; i += 32) { UI[i] = 1.0 / U[i * d + i]; UI32[i] = 1.0f / U32[i * d + i]; }
-    stage = 11;
+    clk.mark(11);
     // 11. the search keeps exact incremental sums mat c, ZB c, Binter c in int64
     // (|entry| < 2^25, |c| < 2^31, <= 64 terms)
     for (int e = lane; e < d * d; e += 32) bad |= uabs64(MAT[e]) >= (1ull << 25);
@@ -673,14 +868,26 @@ h_done:
     return ST_PENDING;
 }
 
-__global__ void __launch_bounds__(128) k_setup(SetupArgs A)
+// Persistent setup kernel: warps take directions from A.todo through an
+// atomic counter.  N = 32 serves h11 <= 32 with the LLL working set in
+// dynamic shared memory (one LllMem<32> per warp) when A.smem_core is set;
+// otherwise (and for N = 64) the working set is the warp's global scratch.
+template <int N> __global__ void __launch_bounds__(128) k_setup(SetupArgs A)
 {
+#ifdef PFG_EMU
+    unsigned char *smem_raw = nullptr;
+#else
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+#endif
     const int lane = threadIdx.x & 31;
+    SetupScratch *Wg = A.scratch + (blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5));
+    LllMem<N> *S = A.smem_core ? (LllMem<N> *)smem_raw + (threadIdx.x >> 5) : (LllMem<N> *)&Wg->core;
     for (;;) {
-        unsigned pid = 0;
-        if (lane == 0) pid = atomicAdd(A.next, 1u);
-        pid = __shfl_sync(FULL, pid, 0);
-        if (pid >= (unsigned)A.n) break;
+        unsigned t = 0;
+        if (lane == 0) t = atomicAdd(A.next, 1u);
+        t = __shfl_sync(FULL, t, 0);
+        if (t >= (unsigned)A.n) break;
+        const int pid = A.todo ? A.todo[t] : (int)t;
         const Geo g = A.geo[A.pgeo[pid]];
         if (lane == 0) {
             Dir &D = A.dirs[pid];
@@ -689,7 +896,7 @@ __global__ void __launch_bounds__(128) k_setup(SetupArgs A)
         }
         __syncwarp();
         int stage = 0;
-        int st = setup_one(A, (int)pid, lane, stage);
+        int st = g.h <= N ? setup_one<N>(A, pid, lane, stage, S) : ST_OVERFLOW;
         if (lane == 0) { A.dirs[pid].status = st; A.dirs[pid].pad = st < 0 ? stage : 0; }
         __syncwarp();
     }

@@ -61,10 +61,17 @@ extern "C" int emu_coni_batch(const pfg_input *in, int precision, int n_warps, p
     const int setup_warps = 4;
     std::vector<SetupScratch> scratch(setup_warps);
     unsigned next = 0;
+    // the device's split: h11 <= 32 through the LllMem<32> kernel, the rest through LllMem<64>
+    std::vector<int32_t> o32, o64;
+    for (int k = 0; k < nb; ++k) (geos[pgeo[k]].h <= 32 ? o32 : o64).push_back(k);
+    unsigned next64 = 0;
     SetupArgs SA{geos.data(), in->kappa, in->Mbasis, in->ps, pgeo.data(), slab_off.data(), slab.data(),
-                 dirs.data(), scratch.data(), nb, &next};
+                 dirs.data(), scratch.data(), (int)o32.size(), &next, o32.data(), 0};
+    SetupArgs SA64 = SA;
+    SA64.n = (int)o64.size(); SA64.next = &next64; SA64.todo = o64.data();
     fprintf(stderr, "emu: setup\n");
-    launch(setup_warps, [&] { k_setup(SA); });
+    if (!o32.empty()) launch(setup_warps, [&] { k_setup<32>(SA); });
+    if (!o64.empty()) launch(setup_warps, [&] { k_setup<MH>(SA64); });
     fprintf(stderr, "emu: setup done\n");
 
     const unsigned long long pts_cap = 1 << 20;
