@@ -251,8 +251,11 @@ def main():
     form = gpu.FORM_PLAIN if args.form == "plain" else gpu.FORM_BATCHED
     prec = gpu.PREC_FP64 if args.precision == "fp64" else gpu.PREC_AUTO
 
-    # work unit: FP64-pruned tree nodes, counted once (untimed)
-    r64 = gpu.coni_batch_multi_ex(geoms, ps, pgeo, device=device, precision=gpu.PREC_FP64)
+    # work unit: nodes of the FP64-pruned tree with every GCD-cut row built (the
+    # reference's pruning), counted once, untimed; the timed steps build the
+    # rows only where they pay off, which changes time but not the points
+    r64 = gpu.coni_batch_multi_ex(geoms, ps, pgeo, device=device, precision=gpu.PREC_FP64,
+                                  gcd_min_tree=-1.0)
     nodes_fp64 = r64[6]["nodes"]
     n_points = len(r64[2])
     for _ in range(args.warmup):

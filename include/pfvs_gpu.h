@@ -85,6 +85,10 @@ typedef struct {
     int precision;             /* PFG_PREC_* */
     int blocks_per_sm;         /* persistent search grid (0: default) */
     int warps_per_block;       /* (0: default) */
+    double gcd_min_tree;       /* GCD-cut rows are built for a direction whose estimated
+                                  search tree has at least this many nodes (they only
+                                  prune; results are identical either way).  0: the
+                                  library default; < 0: always (the reference's pruning) */
 } pfg_options;
 
 /* Statistics of one call. */

@@ -4,7 +4,7 @@
 //   k_search<f>  FP32-pruned persistent search            (pfg_search.cuh)
 //   k_flip       FP32 successes -> done; -11 -> FP64 retry
 //   k_search<d>  FP64-pruned search of the rest
-//   k_expand .. k_gather   canonical output               (pfg_out.cuh)
+//   k_count .. k_rows      canonical output rows              (pfg_out.cuh)
 // with one host synchronisation at the end of a batch (point count, output
 // size).  No CPU fallback: a direction the device cannot finish exactly is
 // reported with a negative status.
@@ -51,8 +51,8 @@ __global__ void k_fill_i32(int32_t *a, int32_t v, int n)
 
 enum {
     W_GEO, W_KAPPA, W_MB, W_PS, W_PGEO, W_SLABOFF, W_SLAB, W_DIRS, W_SCRATCH, W_TODO32, W_TODOALL, W_ORDER,
-    W_CTL, W_ITEMS, W_READY, W_HDR, W_COORDS, W_DIRNODES, W_DIRPASS, W_MFULL, W_KNFULL,
-    W_DIRERR, W_COUNT, W_FILL, W_SEG, W_IDX, W_PAD, W_OM, W_OK, W_OQ, W_OP, W_RETRY, W_N
+    W_CTL, W_ITEMS, W_READY, W_HDR, W_COORDS, W_DIRNODES, W_DIRPASS,
+    W_KEYS, W_COUNT, W_FILL, W_SEG, W_IDX, W_PAD, W_OM, W_OK, W_OQ, W_OP, W_RETRY, W_N
 };
 
 struct Workspace {
@@ -97,6 +97,90 @@ void ws_release(Workspace &W)
     }
 }
 
+// Pinned host blocks for the output arrays handed to the caller: the rows
+// come back by DMA at full link speed, and pfg_output_free returns a block
+// to an idle list for the next call instead of unpinning it.
+struct PinnedPool {
+    std::mutex mu;
+    std::map<void *, size_t> live;              // handed out: block -> capacity
+    std::multimap<size_t, void *> idle;         // capacity -> block
+    size_t idle_bytes = 0;
+};
+constexpr size_t PINNED_IDLE_MAX = 24ull << 30;
+
+PinnedPool &pinned()
+{
+    static PinnedPool *P = new PinnedPool();
+    return *P;
+}
+
+void *pinned_get(size_t bytes)
+{
+    bytes = std::max<size_t>(bytes, 64);
+    PinnedPool &P = pinned();
+    {
+        std::lock_guard<std::mutex> g(P.mu);
+        auto it = P.idle.lower_bound(bytes);
+        if (it != P.idle.end() && it->first <= 2 * bytes + (1u << 20)) {
+            void *p = it->second;
+            P.live[p] = it->first;
+            P.idle_bytes -= it->first;
+            P.idle.erase(it);
+            return p;
+        }
+    }
+    void *p = nullptr;
+    if (cudaHostAlloc(&p, bytes, cudaHostAllocPortable) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    std::lock_guard<std::mutex> g(P.mu);
+    P.live[p] = bytes;
+    return p;
+}
+
+// false if p is not a pinned block of this pool
+bool pinned_put(void *p)
+{
+    if (!p) return true;
+    PinnedPool &P = pinned();
+    size_t cap;
+    {
+        std::lock_guard<std::mutex> g(P.mu);
+        auto it = P.live.find(p);
+        if (it == P.live.end()) return false;
+        cap = it->second;
+        P.live.erase(it);
+        if (P.idle_bytes + cap <= PINNED_IDLE_MAX) {
+            P.idle.emplace(cap, p);
+            P.idle_bytes += cap;
+            return true;
+        }
+    }
+    cudaFreeHost(p);
+    return true;
+}
+
+void pinned_release_idle()
+{
+    PinnedPool &P = pinned();
+    std::multimap<size_t, void *> idle;
+    {
+        std::lock_guard<std::mutex> g(P.mu);
+        idle.swap(P.idle);
+        P.idle_bytes = 0;
+    }
+    for (auto &e : idle) cudaFreeHost(e.second);
+}
+
+struct Chunk { int64_t *M, *Kn, *q, *pidx; size_t n; };
+
+void chunk_free(Chunk &c)
+{
+    for (int64_t *p : {c.M, c.Kn, c.q, c.pidx}) pinned_put(p);
+    c = Chunk{nullptr, nullptr, nullptr, nullptr, 0};
+}
+
 void set_err(pfg_output *out, const char *fmt, ...)
 {
     va_list ap;
@@ -133,7 +217,9 @@ extern "C" int pfg_device_count(void)
 
 extern "C" void pfg_output_free(pfg_output *out)
 {
-    free(out->M); free(out->Kn); free(out->q); free(out->pidx); free(out->pstat);
+    for (int64_t *p : {out->M, out->Kn, out->q, out->pidx})
+        if (!pinned_put(p)) free(p);
+    free(out->pstat);
     out->M = out->Kn = out->q = out->pidx = nullptr;
     out->pstat = nullptr;
     out->n = 0;
@@ -144,6 +230,7 @@ extern "C" void pfg_release(int device)
     Workspace &W = workspace(device);
     std::lock_guard<std::mutex> g(W.mu);
     if (cudaSetDevice(device) == cudaSuccess) ws_release(W);
+    pinned_release_idle();
 }
 
 extern "C" int pfg_coni_batch(const pfg_input *in, pfg_output *out)
@@ -156,8 +243,10 @@ extern "C" int pfg_coni_batch_ex(const pfg_input *in, const pfg_options *opt_in,
 {
     memset(out, 0, sizeof *out);
     if (stats) memset(stats, 0, sizeof *stats);
-    pfg_options opt = {PFG_FORM_BATCHED, PFG_PREC_AUTO, 0, 0};
+    pfg_options opt = {PFG_FORM_BATCHED, PFG_PREC_AUTO, 0, 0, 0.0};
     if (opt_in) opt = *opt_in;
+    const double gcd_min_tree = opt.gcd_min_tree == 0.0 ? GCD_MIN_TREE_DEFAULT
+                                : (opt.gcd_min_tree < 0.0 ? 0.0 : opt.gcd_min_tree);
     const int64_t NP = in->n_p;
     if (NP < 0 || in->n_geo < 0) { set_err(out, "negative sizes"); return 1; }
     std::vector<Geo> geos(in->n_geo);
@@ -192,7 +281,7 @@ extern "C" int pfg_coni_batch_ex(const pfg_input *in, const pfg_options *opt_in,
     int64_t launches = 0;
     Workspace &W = workspace(in->device);
     std::unique_lock<std::mutex> lock(W.mu);
-    std::vector<int64_t> Mo, Ko, qo, po;
+    std::vector<Chunk> chunks;
     cudaEvent_t ev[8] = {};
     int64_t koff_total = 0, moff_total = 0;
     Geo *dgeo = nullptr;
@@ -297,13 +386,13 @@ extern "C" int pfg_coni_batch_ex(const pfg_input *in, const pfg_options *opt_in,
                 unsigned *counters = (unsigned *)((char *)dctl + 2 * sizeof(SearchCtl));
                 if (n32) {
                     SetupArgs SA{dgeo, dkappa, dmb, dps, dpgeo, dslaboff, dslab, ddirs, dscr, n32,
-                                 counters, dorder, 1};
+                                 counters, dorder, 1, gcd_min_tree};
                     k_setup<32><<<grid32, 32, smem32>>>(SA); ++launches;
                     CK(cudaGetLastError());
                 }
                 if (n64) {
                     SetupArgs SA{dgeo, dkappa, dmb, dps, dpgeo, dslaboff, dslab, ddirs, dscr, n64,
-                                 counters + 1, dorder + n32, 0};
+                                 counters + 1, dorder + n32, 0, gcd_min_tree};
                     k_setup<MH><<<grid64, 128>>>(SA); ++launches;
                     CK(cudaGetLastError());
                 }
@@ -368,29 +457,22 @@ extern "C" int pfg_coni_batch_ex(const pfg_input *in, const pfg_options *opt_in,
                 goto restart_search;
             }
             // ---- output ----
-            int64_t *dM, *dK; int *derr; unsigned *dcount, *dfill, *didx, *dpad; unsigned long long *dseg;
-            WS(dM, W_MFULL, std::max<unsigned long long>(npts, 1) * MH * 8);
-            WS(dK, W_KNFULL, std::max<unsigned long long>(npts, 1) * MH * 8);
-            WS(derr, W_DIRERR, (size_t)nb * 4);
+            unsigned *dcount, *dfill, *didx, *dpad; unsigned long long *dseg; int64_t *dkeys;
             WS(dcount, W_COUNT, (size_t)nb * 4);
             WS(dfill, W_FILL, (size_t)nb * 4);
             WS(dseg, W_SEG, (size_t)(nb + 1) * 8);
             WS(didx, W_IDX, std::max<unsigned long long>(npts, 1) * 4);
-            WS(dpad, W_PAD, std::max<unsigned long long>(npts, 1) * 8 + 64);
-            CK(cudaMemset(derr, 0, (size_t)nb * 4));
+            WS(dpad, W_PAD, std::max<unsigned long long>(npts, 1) * 8 + 256);
+            int ks = 3;
+            for (int k = 0; k < nb; ++k) ks = std::max(ks, geos[in->pgeo[off + k]].h);
+            WS(dkeys, W_KEYS, std::max<unsigned long long>(npts, 1) * ks * 8);
             CK(cudaMemset(dcount, 0, (size_t)nb * 4));
             CK(cudaMemset(dfill, 0, (size_t)nb * 4));
             CK(cudaEventRecord(ev[3]));
-            OutArgs O{ddirs, dslab, dhdr, dcoords, ddirpass, npts, nb, dM, dK, derr, dcount, dfill, dseg, didx};
-            if (npts) {
-                k_expand<<<nsm * 8, 256>>>(O); ++launches;
-                k_count<<<nsm * 4, 256>>>(O); ++launches;
-            }
+            OutArgs O{ddirs, dslab, dhdr, dcoords, ddirpass, npts, nb, dcount, dfill, dseg, didx, dkeys, ks, dpad};
+            if (npts) { k_count<<<nsm * 4, 256>>>(O); ++launches; }
             k_scan<<<1, 1024>>>(O); ++launches;
-            if (npts) {
-                k_scatter<<<nsm * 4, 256>>>(O); ++launches;
-                k_segsort<<<std::min(nb, nsm * 8), 256>>>(O, dpad); ++launches;
-            }
+            if (npts) { k_scatter<<<nsm * 4, 256>>>(O); ++launches; }
             CK(cudaGetLastError());
             unsigned long long n_out = 0;
             CK(cudaMemcpy(&n_out, dseg + nb, 8, cudaMemcpyDeviceToHost));
@@ -400,30 +482,32 @@ extern "C" int pfg_coni_batch_ex(const pfg_input *in, const pfg_options *opt_in,
             WS(oq, W_OQ, std::max<unsigned long long>(n_out, 1) * 8);
             WS(op, W_OP, std::max<unsigned long long>(n_out, 1) * 8);
             if (n_out) {
-                GatherArgs G{didx, dhdr, dM, dK, n_out, off, oM, oK, oq, op};
-                k_gather<<<nsm * 8, 256>>>(G); ++launches;
+                const int smem_sort = SORT_CAP * KEYN * 8 + SORT_CAP * 4;
+                CK(cudaFuncSetAttribute(k_segsort, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_sort));
+                k_keys<<<nsm * 4, 256>>>(O, n_out); ++launches;
+                k_segsort<<<std::min(nb, nsm * 3), 256, smem_sort>>>(O); ++launches;
+                RowArgs R{ddirs, dslab, dhdr, dcoords, didx, n_out, off, oM, oK, oq, op};
+                k_rows<<<nsm * 8, 256>>>(R); ++launches;
                 CK(cudaGetLastError());
             }
             CK(cudaEventRecord(ev[4]));
-            const size_t base = qo.size();
-            Mo.resize((base + n_out) * MH); Ko.resize((base + n_out) * MH);
-            qo.resize(base + n_out); po.resize(base + n_out);
             if (n_out) {
-                CK(cudaMemcpy(&Mo[base * MH], oM, n_out * MH * 8, cudaMemcpyDeviceToHost));
-                CK(cudaMemcpy(&Ko[base * MH], oK, n_out * MH * 8, cudaMemcpyDeviceToHost));
-                CK(cudaMemcpy(&qo[base], oq, n_out * 8, cudaMemcpyDeviceToHost));
-                CK(cudaMemcpy(&po[base], op, n_out * 8, cudaMemcpyDeviceToHost));
+                Chunk c{(int64_t *)pinned_get(n_out * MH * 8), (int64_t *)pinned_get(n_out * MH * 8),
+                        (int64_t *)pinned_get(n_out * 8), (int64_t *)pinned_get(n_out * 8), (size_t)n_out};
+                chunks.push_back(c);
+                if (!c.M || !c.Kn || !c.q || !c.pidx) { set_err(out, "out of pinned host memory"); rc = 1; goto fail; }
+                CK(cudaMemcpy(c.M, oM, n_out * MH * 8, cudaMemcpyDeviceToHost));
+                CK(cudaMemcpy(c.Kn, oK, n_out * MH * 8, cudaMemcpyDeviceToHost));
+                CK(cudaMemcpy(c.q, oq, n_out * 8, cudaMemcpyDeviceToHost));
+                CK(cudaMemcpy(c.pidx, op, n_out * 8, cudaMemcpyDeviceToHost));
             }
             // statuses
             {
                 std::vector<Dir> hd(nb);
-                std::vector<int> herr(nb);
                 CK(cudaMemcpy(hd.data(), ddirs, (size_t)nb * sizeof(Dir), cudaMemcpyDeviceToHost));
-                CK(cudaMemcpy(herr.data(), derr, (size_t)nb * 4, cudaMemcpyDeviceToHost));
                 std::map<std::pair<int, int>, int> fails;
                 for (int k = 0; k < nb; ++k) {
-                    int st = hd[k].status;
-                    if (herr[k]) st = ST_OVERFLOW;
+                    const int st = hd[k].status;
                     out->pstat[off + k] = (st == ST_OK || st == ST_PENDING || st == ST_EMPTY) ? 0 : (int8_t)st;
                     if (out->pstat[off + k]) fails[{st, hd[k].pad}]++;
                 }
@@ -465,21 +549,32 @@ extern "C" int pfg_coni_batch_ex(const pfg_input *in, const pfg_options *opt_in,
         }
     }
     {
-        const size_t n = qo.size();
+        size_t n = 0;
+        for (auto &c : chunks) n += c.n;
         out->n = (int64_t)n;
-        out->M = (int64_t *)malloc(n * MH * 8 + 8);
-        out->Kn = (int64_t *)malloc(n * MH * 8 + 8);
-        out->q = (int64_t *)malloc(n * 8 + 8);
-        out->pidx = (int64_t *)malloc(n * 8 + 8);
-        if (!out->M || !out->Kn || !out->q || !out->pidx) { set_err(out, "out of host memory"); rc = 1; goto fail; }
-        if (n) {
-            memcpy(out->M, Mo.data(), n * MH * 8);
-            memcpy(out->Kn, Ko.data(), n * MH * 8);
-            memcpy(out->q, qo.data(), n * 8);
-            memcpy(out->pidx, po.data(), n * 8);
+        if (chunks.size() == 1) {
+            out->M = chunks[0].M; out->Kn = chunks[0].Kn; out->q = chunks[0].q; out->pidx = chunks[0].pidx;
+            chunks.clear();
+        } else {
+            out->M = (int64_t *)pinned_get(n * MH * 8);
+            out->Kn = (int64_t *)pinned_get(n * MH * 8);
+            out->q = (int64_t *)pinned_get(n * 8);
+            out->pidx = (int64_t *)pinned_get(n * 8);
+            if (!out->M || !out->Kn || !out->q || !out->pidx) { set_err(out, "out of pinned host memory"); rc = 1; goto fail; }
+            size_t base = 0;
+            for (auto &c : chunks) {
+                memcpy(out->M + base * MH, c.M, c.n * MH * 8);
+                memcpy(out->Kn + base * MH, c.Kn, c.n * MH * 8);
+                memcpy(out->q + base, c.q, c.n * 8);
+                memcpy(out->pidx + base, c.pidx, c.n * 8);
+                base += c.n;
+                chunk_free(c);
+            }
+            chunks.clear();
         }
     }
 fail:
+    for (auto &c : chunks) chunk_free(c);
     for (auto &e : ev) if (e) cudaEventDestroy(e);
     if (rc) {
         cudaGetLastError();

@@ -80,6 +80,8 @@ struct SetupArgs {
     unsigned *next;                         // work counter
     const int32_t *todo;                    // directions to set up (null: 0..n-1)
     int smem_core;                          // 1: the LllMem<32> lives in dynamic shared memory
+    double gcd_min_tree;                    // GCD rows only for trees estimated at >= this many
+                                            // nodes (<= 0: always)
 };
 
 // Per-stage cycle accounting of the setup, compiled in only with
@@ -709,93 +711,6 @@ template <int N> __device__ int setup_one(const SetupArgs &A, int pid, int lane,
         return ST_EMPTY;
     }
 
-    clk.mark(9);
-    // 9. GCD rows: echelon basis of the row lattice of ZB[1:] with small rows.
-    // The rows r_k = ZB[k][:], k = 1..d, satisfy sum_k p_k r_k = 0 (p^T Z Binter
-    // = 0 and p_0 = 0); with V p' = e0 from Bezout steps, the rows of V^-T R
-    // are the rows of R with row 0 = p'^T R = 0: drop it, the rest is a basis.
-    // (Lanes own columns here, so the row operations need no staging.)
-    for (int c = lane; c < d; c += 32)
-        for (int r = 0; r < d; ++r) S->B[r * N + c] = ZT[c * h + r + 1];
-    for (int e = lane; e < d; e += 32) W->w[e] = p[e + 1];
-    __syncwarp();
-    for (int k = 1; k < d; ++k) {
-        int64_t wk = W->w[k];
-        if (wk == 0) continue;
-        int64_t w0 = W->w[0], s, t;
-        int64_t gg = xgcd_floor(w0, wk, &s, &t);
-        int64_t m10 = -fdiv64(wk, gg), m11 = fdiv64(w0, gg);
-        __syncwarp();
-        if (lane == 0) { W->w[0] = gg; W->w[k] = 0; }
-        for (int c = lane; c < d; c += 32) {
-            i128 r0 = (i128)m11 * S->B[c] - (i128)m10 * S->B[k * N + c];
-            i128 rk = -(i128)t * S->B[c] + (i128)s * S->B[k * N + c];
-            if (!fits64(r0) || !fits64(rk)) { bad = true; continue; }
-            S->B[c] = (int64_t)r0;
-            S->B[k * N + c] = (int64_t)rk;
-        }
-        __syncwarp();
-        if (warp_any(bad)) return ST_OVERFLOW;
-    }
-    clk.mark(91);
-    for (int c = lane; c < d; c += 32) bad |= S->B[c] != 0;
-    if (warp_any(bad)) return ST_OVERFLOW;          // p'^T ZB[1:] must vanish exactly
-    int64_t *H = slab + L.H;
-    for (int e = lane; e < d * d; e += 32) H[e] = 0;
-    uint64_t hrows = 0;
-    {
-        int nr = d - 1;
-        for (int c = lane; c < d; c += 32)          // drop row 0
-            for (int r = 0; r < nr; ++r) S->B[r * N + c] = S->B[(r + 1) * N + c];
-        __syncwarp();
-        // Rows whose construction would leave int64 (the last pivots are
-        // large: the lattice of rows vanishing on all but the last columns has
-        // a huge covolume) are not built: the rows found so far are kept, and
-        // any set of rows of the lattice gives a valid GCD bound.
-        if (nr > 0) {
-            if (gram_euclid<N>(S, nr, d, lane)) goto h_done;
-            Lll<N> LH{S, d, nr};
-            if (warp_lll(LH, nr, false, PFG_DELTA_H, lane)) goto h_done;
-            for (int col = 0; col < d && nr > 0; ++col) {
-                int pr = -1;
-                LH.M = nr;
-                for (int it = 0; ; ++it) {
-                    if (it > 256) goto h_done;
-                    pr = argmin_nonzero<N>(S->B, nr, col, lane);
-                    PFG_UNIFORM(pr);
-                    if (pr < 0) break;
-                    bool other = false;
-                    for (int r = lane; r < nr; r += 32) other |= r != pr && S->B[r * N + col] != 0;
-                    if (!warp_any(other)) break;
-                    if (echelon_step(LH, nr, pr, col, lane)) goto h_done;
-                }
-                if (pr < 0) continue;
-                // the pivot row to the end (index nr - 1), positive pivot
-                lll_exchange(LH, pr, nr - 1, lane);
-                const bool neg = S->B[(nr - 1) * N + col] < 0;
-                PFG_UNIFORM(neg);
-                __syncwarp();                   // (read by every lane before the owner negates it)
-                if (neg) {
-                    for (int c = lane; c < d; c += 32) S->B[(nr - 1) * N + c] = -S->B[(nr - 1) * N + c];
-                    for (int l = lane; l < nr - 1; l += 32) S->G[gix(nr - 1, l)] = -S->G[gix(nr - 1, l)];
-                    __syncwarp();
-                }
-                // LLL the rows below (rows 0..nr-2), size-reduce the pivot row against them
-                if (warp_lll(LH, nr - 1, true, PFG_DELTA_H, lane)) goto h_done;
-                bool fits = true;
-                for (int c = lane; c < d; c += 32) fits &= uabs64(S->B[(nr - 1) * N + c]) < (1ull << 62);
-                fits = __all_sync(FULL, fits);
-                if (fits) {
-                    for (int c = lane; c < d; c += 32) H[col * d + c] = S->B[(nr - 1) * N + c];
-                    hrows |= 1ull << col;
-                }
-                __syncwarp();
-                --nr;
-            }
-        }
-    }
-h_done:
-
     clk.mark(10);
     // 10. FP64 Cholesky of mat, certificate, float copies
     double *U = (double *)(slab + L.u64);
@@ -852,6 +767,121 @@ h_done:
     for (int e = lane; e < d * d; e += 32) U32[e] = (float)U[e];
     __syncwarp();
     for (int i = lane; i < d; i += 32) { UI[i] = 1.0 / U[i * d + i]; UI32[i] = 1.0f / U32[i * d + i]; }
+    // Tree estimate (Gaussian heuristic): the points of the projected lattice
+    // of the last k coordinates inside the ellipsoid's shadow, summed over k.
+    // The GCD rows below only prune, so a direction whose tree is small
+    // (or whose root interval is empty) is searched without them: building
+    // them costs more than they could save there.
+    bool want_rows = A.gcd_min_tree <= 0.0;
+    if (!want_rows) {
+        double est = 0.0;
+        if (lane == 0) {
+            const double lq = log((double)g.qmax + 1.0) + 1.1447298858494002;   // + log(pi)
+            double ldet = 0.0;
+            for (int k = 1; k <= d; ++k) {
+                ldet += log(U[(d - k) * d + (d - k)]);
+                est += exp(0.5 * k * lq - lgamma(0.5 * k + 1.0) - ldet);
+            }
+            if (m0_level == d - 1 && g.linmin > 0) {          // root interval under the M0 cut
+                const double rmax = sqrt((double)g.qmax + slack_chol + 1.0) / U[(d - 1) * d + (d - 1)];
+                const double cmin = ceil((double)g.linmin / fabs((double)g_lin));
+                if (cmin > rmax * (1.0 + 1e-9) + 1e-9) est = 0.0;
+            }
+        }
+        est = __shfl_sync(FULL, est, 0);
+        want_rows = est >= A.gcd_min_tree;
+    }
+    int64_t *H = slab + L.H;
+    for (int e = lane; e < d * d; e += 32) H[e] = 0;
+    uint64_t hrows = 0;
+    clk.mark(9);
+    // 9. GCD rows: echelon basis of the row lattice of ZB[1:] with small rows.
+    // The rows r_k = ZB[k][:], k = 1..d, satisfy sum_k p_k r_k = 0 (p^T Z Binter
+    // = 0 and p_0 = 0); with V p' = e0 from Bezout steps, the rows of V^-T R
+    // are the rows of R with row 0 = p'^T R = 0: drop it, the rest is a basis.
+    // (Lanes own columns here, so the row operations need no staging.)  The
+    // rows only prune: when one cannot be built, the search goes without it.
+    if (want_rows) {
+        for (int c = lane; c < d; c += 32)
+            for (int r = 0; r < d; ++r) S->B[r * N + c] = ZT[c * h + r + 1];
+        for (int e = lane; e < d; e += 32) W->w[e] = p[e + 1];
+        __syncwarp();
+        for (int k = 1; k < d; ++k) {
+            int64_t wk = W->w[k];
+            if (wk == 0) continue;
+            int64_t w0 = W->w[0], s, t;
+            int64_t gg = xgcd_floor(w0, wk, &s, &t);
+            int64_t m10 = -fdiv64(wk, gg), m11 = fdiv64(w0, gg);
+            __syncwarp();
+            if (lane == 0) { W->w[0] = gg; W->w[k] = 0; }
+            for (int c = lane; c < d; c += 32) {
+                i128 r0 = (i128)m11 * S->B[c] - (i128)m10 * S->B[k * N + c];
+                i128 rk = -(i128)t * S->B[c] + (i128)s * S->B[k * N + c];
+                if (!fits64(r0) || !fits64(rk)) { bad = true; continue; }
+                S->B[c] = (int64_t)r0;
+                S->B[k * N + c] = (int64_t)rk;
+            }
+            __syncwarp();
+            if (warp_any(bad)) { bad = false; want_rows = false; break; }
+        }
+    }
+    clk.mark(91);
+    if (want_rows) {
+        for (int c = lane; c < d; c += 32) bad |= S->B[c] != 0;
+        if (warp_any(bad)) return ST_OVERFLOW;      // p'^T ZB[1:] must vanish exactly
+    }
+    if (want_rows) {
+        int nr = d - 1;
+        for (int c = lane; c < d; c += 32)          // drop row 0
+            for (int r = 0; r < nr; ++r) S->B[r * N + c] = S->B[(r + 1) * N + c];
+        __syncwarp();
+        // Rows whose construction would leave int64 (the last pivots are
+        // large: the lattice of rows vanishing on all but the last columns has
+        // a huge covolume) are not built: the rows found so far are kept, and
+        // any set of rows of the lattice gives a valid GCD bound.
+        if (nr > 0) {
+            if (gram_euclid<N>(S, nr, d, lane)) goto h_done;
+            Lll<N> LH{S, d, nr};
+            if (warp_lll(LH, nr, false, PFG_DELTA_H, lane)) goto h_done;
+            for (int col = 0; col < d && nr > 0; ++col) {
+                int pr = -1;
+                LH.M = nr;
+                for (int it = 0; ; ++it) {
+                    if (it > 256) goto h_done;
+                    pr = argmin_nonzero<N>(S->B, nr, col, lane);
+                    PFG_UNIFORM(pr);
+                    if (pr < 0) break;
+                    bool other = false;
+                    for (int r = lane; r < nr; r += 32) other |= r != pr && S->B[r * N + col] != 0;
+                    if (!warp_any(other)) break;
+                    if (echelon_step(LH, nr, pr, col, lane)) goto h_done;
+                }
+                if (pr < 0) continue;
+                // the pivot row to the end (index nr - 1), positive pivot
+                lll_exchange(LH, pr, nr - 1, lane);
+                const bool neg = S->B[(nr - 1) * N + col] < 0;
+                PFG_UNIFORM(neg);
+                __syncwarp();                   // (read by every lane before the owner negates it)
+                if (neg) {
+                    for (int c = lane; c < d; c += 32) S->B[(nr - 1) * N + c] = -S->B[(nr - 1) * N + c];
+                    for (int l = lane; l < nr - 1; l += 32) S->G[gix(nr - 1, l)] = -S->G[gix(nr - 1, l)];
+                    __syncwarp();
+                }
+                // LLL the rows below (rows 0..nr-2), size-reduce the pivot row against them
+                if (warp_lll(LH, nr - 1, true, PFG_DELTA_H, lane)) goto h_done;
+                bool fits = true;
+                for (int c = lane; c < d; c += 32) fits &= uabs64(S->B[(nr - 1) * N + c]) < (1ull << 62);
+                fits = __all_sync(FULL, fits);
+                if (fits) {
+                    for (int c = lane; c < d; c += 32) H[col * d + c] = S->B[(nr - 1) * N + c];
+                    hrows |= 1ull << col;
+                }
+                __syncwarp();
+                --nr;
+            }
+        }
+    }
+h_done:
     clk.mark(11);
     // 11. the search keeps exact incremental sums mat c, ZB c, Binter c in int64
     // (|entry| < 2^25, |c| < 2^31, <= 64 terms)

@@ -9,6 +9,11 @@ constexpr int MH = 64;          // largest h11 (pfg_max_h11)
 constexpr int MD = MH - 1;      // largest search dimension
 constexpr unsigned FULL = 0xffffffffu;
 
+// A direction gets GCD rows (pruning only) when its estimated search tree
+// has at least this many nodes: below that, building the rows costs more
+// device time than the nodes they could remove.
+constexpr double GCD_MIN_TREE_DEFAULT = 1.0e3;
+
 // per-direction status (device); the ABI's pstat carries the same codes
 enum : int {
     ST_OK = 0,          // searched, points emitted

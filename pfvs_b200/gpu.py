@@ -46,7 +46,8 @@ class _Output(ctypes.Structure):
 
 class _Options(ctypes.Structure):
     _fields_ = [("form", ctypes.c_int), ("precision", ctypes.c_int),
-                ("blocks_per_sm", ctypes.c_int), ("warps_per_block", ctypes.c_int)]
+                ("blocks_per_sm", ctypes.c_int), ("warps_per_block", ctypes.c_int),
+                ("gcd_min_tree", ctypes.c_double)]
 
 
 class _Stats(ctypes.Structure):
@@ -174,9 +175,32 @@ def _pack(geoms, ps, pgeo, MH):
     return h, Q, qmax, linmin, kap, Mb, P, pgeo, n_p
 
 
+class _OutputOwner:
+    """Owns one pfg_output; frees it (pfg_output_free) when collected."""
+
+    def __init__(self, lib, out):
+        self.lib, self.out = lib, out
+
+    def __del__(self):
+        try:
+            self.lib.pfg_output_free(ctypes.byref(self.out))
+        except Exception:
+            pass
+
+
+def _view(owner, ptr, shape):
+    """int64 array of `shape` over the library buffer at `ptr`, keeping `owner` alive."""
+    n = int(np.prod(shape))
+    if n == 0:
+        return np.zeros(shape, dtype=np.int64)
+    buf = (ctypes.c_int64 * n).from_address(ctypes.cast(ptr, ctypes.c_void_p).value)
+    buf._owner = owner
+    return np.ctypeslib.as_array(buf).reshape(shape)
+
+
 def coni_batch_multi_ex(geoms, ps, pgeo, device=0, batch=0, verbose=False,
                         form=FORM_BATCHED, precision=PREC_AUTO, blocks_per_sm=0,
-                        warps_per_block=0, want_dir_nodes=False):
+                        warps_per_block=0, want_dir_nodes=False, gcd_min_tree=0.0):
     """
     `coni_batch_multi` with the search form (FORM_BATCHED: one persistent
     work-stealing launch; FORM_PLAIN: one launch per direction), the pruning
@@ -192,7 +216,7 @@ def coni_batch_multi_ex(geoms, ps, pgeo, device=0, batch=0, verbose=False,
                  kap.ctypes.data_as(_i64p), Mb.ctypes.data_as(_i64p),
                  n_p, P.ctypes.data_as(_i64p), pgeo.ctypes.data_as(_i32p),
                  int(device), int(batch), int(bool(verbose)))
-    opt = _Options(int(form), int(precision), int(blocks_per_sm), int(warps_per_block))
+    opt = _Options(int(form), int(precision), int(blocks_per_sm), int(warps_per_block), float(gcd_min_tree))
     st = _Stats()
     dn = np.zeros(max(n_p, 1), dtype=np.int64)
     out = _Output()
@@ -200,20 +224,16 @@ def coni_batch_multi_ex(geoms, ps, pgeo, device=0, batch=0, verbose=False,
                                ctypes.byref(st), dn.ctypes.data_as(_i64p))
     if rc != 0:
         raise RuntimeError(f"GPU pipeline failed: {out.err.decode(errors='replace')}")
-    try:
-        n = out.n
-
-        def arr(ptr, shape):
-            if n == 0:
-                return np.zeros(shape, dtype=np.int64)
-            return np.ctypeslib.as_array(ptr, shape=shape).copy()
-        M, Kn = arr(out.M, (n, MH)), arr(out.Kn, (n, MH))
-        q, pidx = arr(out.q, (n,)), arr(out.pidx, (n,))
-        pstat = np.ctypeslib.as_array(out.pstat, shape=(n_p,)).copy() if n_p \
-            else np.zeros(0, dtype=np.int8)
-        secs = out.seconds_gpu
-    finally:
-        lib.pfg_output_free(ctypes.byref(out))
+    # The row arrays view the library's (pinned) output buffers without a copy;
+    # the buffers go back to the library when the last view is collected.
+    owner = _OutputOwner(lib, out)
+    n = out.n
+    M, Kn = _view(owner, out.M, (n, MH)), _view(owner, out.Kn, (n, MH))
+    q, pidx = _view(owner, out.q, (n,)), _view(owner, out.pidx, (n,))
+    pstat = np.ctypeslib.as_array(out.pstat, shape=(n_p,)).copy() if n_p \
+        else np.zeros(0, dtype=np.int8)
+    secs = out.seconds_gpu
+    del owner
     res = (M, Kn, q, pidx, pstat.astype(np.int8), secs, st.as_dict())
     return res + (dn[:n_p],) if want_dir_nodes else res
 

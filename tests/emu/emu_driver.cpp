@@ -66,7 +66,7 @@ extern "C" int emu_coni_batch(const pfg_input *in, int precision, int n_warps, p
     for (int k = 0; k < nb; ++k) (geos[pgeo[k]].h <= 32 ? o32 : o64).push_back(k);
     unsigned next64 = 0;
     SetupArgs SA{geos.data(), in->kappa, in->Mbasis, in->ps, pgeo.data(), slab_off.data(), slab.data(),
-                 dirs.data(), scratch.data(), (int)o32.size(), &next, o32.data(), 0};
+                 dirs.data(), scratch.data(), (int)o32.size(), &next, o32.data(), 0, GCD_MIN_TREE_DEFAULT};
     SetupArgs SA64 = SA;
     SA64.n = (int)o64.size(); SA64.next = &next64; SA64.todo = o64.data();
     fprintf(stderr, "emu: setup\n");
@@ -105,21 +105,17 @@ extern "C" int emu_coni_batch(const pfg_input *in, int precision, int n_warps, p
     if (ctl[0].err || ctl[1].err) { snprintf(out->err, sizeof out->err, "wait ran out"); return 1; }
     const unsigned long long npts = ctl[0].npts;
     if (npts > pts_cap) { snprintf(out->err, sizeof out->err, "point buffer overflow"); return 1; }
-    std::vector<int64_t> Mf(std::max<unsigned long long>(npts, 1) * MH), Kf(std::max<unsigned long long>(npts, 1) * MH);
-    std::vector<int> derr(nb, 0);
-    std::vector<unsigned> cnt(nb, 0), fill(nb, 0), idx(std::max<unsigned long long>(npts, 1)), pad(2 * std::max<unsigned long long>(npts, 1) + 64);
+    std::vector<unsigned> cnt(nb, 0), fill(nb, 0), idx(std::max<unsigned long long>(npts, 1)),
+        pad(2 * std::max<unsigned long long>(npts, 1) + 64);
+    int ks = 3;
+    for (int k = 0; k < nb; ++k) ks = std::max(ks, geos[pgeo[k]].h);
+    std::vector<int64_t> keys(std::max<unsigned long long>(npts, 1) * ks);
     std::vector<unsigned long long> seg(nb + 1, 0);
-    OutArgs O{dirs.data(), slab.data(), hdr.data(), coords.data(), dpass.data(), npts, nb, Mf.data(), Kf.data(),
-              derr.data(), cnt.data(), fill.data(), seg.data(), idx.data()};
-    if (npts) {
-        launch(4, [&] { k_expand(O); });
-        launch(4, [&] { k_count(O); });
-    }
+    OutArgs O{dirs.data(), slab.data(), hdr.data(), coords.data(), dpass.data(), npts, nb,
+              cnt.data(), fill.data(), seg.data(), idx.data(), keys.data(), ks, pad.data()};
+    if (npts) launch(4, [&] { k_count(O); });
     launch(1, [&] { k_scan(O); });
-    if (npts) {
-        launch(4, [&] { k_scatter(O); });
-        launch(std::min(nb, 8), [&] { k_segsort(O, pad.data()); });
-    }
+    if (npts) launch(4, [&] { k_scatter(O); });
     const unsigned long long n_out = seg[nb];
     out->n = (int64_t)n_out;
     out->M = (int64_t *)malloc(n_out * MH * 8 + 8);
@@ -127,12 +123,14 @@ extern "C" int emu_coni_batch(const pfg_input *in, int precision, int n_warps, p
     out->q = (int64_t *)malloc(n_out * 8 + 8);
     out->pidx = (int64_t *)malloc(n_out * 8 + 8);
     if (n_out) {
-        GatherArgs G{idx.data(), hdr.data(), Mf.data(), Kf.data(), n_out, 0, out->M, out->Kn, out->q, out->pidx};
-        launch(4, [&] { k_gather(G); });
+        launch(4, [&] { k_keys(O, n_out); });
+        launch(std::min(nb, 8), [&] { k_segsort(O); });
+        RowArgs R{dirs.data(), slab.data(), hdr.data(), coords.data(), idx.data(), n_out, 0,
+                  out->M, out->Kn, out->q, out->pidx};
+        launch(4, [&] { k_rows(R); });
     }
     for (int k = 0; k < nb; ++k) {
-        int st = dirs[k].status;
-        if (derr[k]) st = ST_OVERFLOW;
+        const int st = dirs[k].status;
         out->pstat[k] = (st == ST_OK || st == ST_PENDING || st == ST_EMPTY) ? 0 : (int8_t)st;
         if (dir_nodes_out) dir_nodes_out[k] = (int64_t)dnodes[k];
         if (dir_debug) dir_debug[k] = dirs[k].pad;

@@ -82,3 +82,45 @@ def test_repeat_calls_identical():
     a = gpu.coni_batch_multi(geoms, ps, pgeo)
     b = gpu.coni_batch_multi(geoms, ps, pgeo)
     assert_same(b, a)
+
+
+def test_gcd_row_policy_keeps_points():
+    """GCD-cut rows only prune: building them for every direction (the
+    reference's pruning), for the large trees only (the default), or for none
+    gives the same points; only the node counts differ."""
+    w = workloads.build("mixed", n_p=4096)
+    geoms, ps, pgeo, _ = layout(w)
+    always = gpu.coni_batch_multi_ex(geoms, ps, pgeo, gcd_min_tree=-1.0)
+    default = gpu.coni_batch_multi_ex(geoms, ps, pgeo)
+    never = gpu.coni_batch_multi_ex(geoms, ps, pgeo, gcd_min_tree=1e30)
+    for x in (default, never):
+        assert_same(x, always)
+        np.testing.assert_array_equal(x[4], always[4])
+    assert always[6]["nodes"] <= default[6]["nodes"] <= never[6]["nodes"]
+    assert always[6]["nodes"] < never[6]["nodes"]
+
+
+def _is_canonical(M, Kn, pidx):
+    """rows strictly increasing in (pidx, M, Kn) lexicographic order"""
+    keys = np.concatenate([pidx[:, None], M, Kn], axis=1)
+    a, b = keys[:-1], keys[1:]
+    diff = a != b
+    first = np.argmax(diff, axis=1)
+    rows = np.arange(len(a))
+    return bool(np.all(diff.any(axis=1)) and np.all(a[rows, first] < b[rows, first]))
+
+
+def test_output_canonical_on_a_large_batch():
+    """Size-independent check at a size the oracle cannot follow: 16,384
+    directions of the mixed batch, including directions with more points
+    than the shared-memory sort holds (the global-memory sort path); the
+    rows come out in the canonical order and equal the plain form's."""
+    w = workloads.build("mixed", n_p=16384)
+    geoms, ps, pgeo, _ = layout(w)
+    a = gpu.coni_batch_multi_ex(geoms, ps, pgeo)
+    M, Kn, q, pidx = a[:4]
+    counts = np.bincount(pidx, minlength=len(ps))
+    assert counts.max() > 2048
+    assert _is_canonical(M, Kn, pidx)
+    b = gpu.coni_batch_multi_ex(geoms, ps, pgeo, precision=gpu.PREC_FP64)
+    assert_same(b, a)
