@@ -52,13 +52,14 @@ __global__ void k_fill_i32(int32_t *a, int32_t v, int n)
 enum {
     W_GEO, W_KAPPA, W_MB, W_PS, W_PGEO, W_SLABOFF, W_SLAB, W_DIRS, W_SCRATCH, W_TODO32, W_TODOALL, W_ORDER,
     W_CTL, W_ITEMS, W_READY, W_HDR, W_COORDS, W_DIRNODES, W_DIRPASS,
-    W_KEYS, W_COUNT, W_FILL, W_SEG, W_IDX, W_PAD, W_OM, W_OK, W_OQ, W_OP, W_RETRY, W_N
+    W_KEYS, W_COUNT, W_FILL, W_SEG, W_IDX, W_CSEG, W_SUM, W_PERM, W_PERM2, W_SIDX, W_OM, W_OK, W_OQ, W_OP, W_RETRY, W_N
 };
 
 struct Workspace {
     std::mutex mu;
     void *p[W_N] = {};
     size_t cap[W_N] = {};
+    unsigned long long pts_cap = 1ull << 20;    // point buffer: grows to the largest batch seen
 };
 
 std::mutex g_ws_mu;
@@ -312,7 +313,7 @@ extern "C" int pfg_coni_batch_ex(const pfg_input *in, const pfg_options *opt_in,
             }
             batch = std::max<int64_t>(1, std::min(batch, nb));
         }
-        unsigned long long pts_cap = 1ull << 20;
+        unsigned long long &pts_cap = W.pts_cap;
         const unsigned q_cap = 1u << 20;
         for (int64_t off = 0; off < NP;) {
             const int nb = (int)std::min<int64_t>(batch, NP - off);
@@ -452,30 +453,44 @@ extern "C" int pfg_coni_batch_ex(const pfg_input *in, const pfg_options *opt_in,
             }
             const unsigned long long npts = hctl[0].npts;
             if (npts > pts_cap) {
+                // the device time of the attempt counts; then again with room for every point
+                float ms_a[2];
+                CK(cudaEventElapsedTime(&ms_a[0], ev[0], ev[1]));
+                CK(cudaEventElapsedTime(&ms_a[1], ev[1], ev[2]));
+                out->seconds_gpu += (ms_a[0] + ms_a[1]) / 1e3;
+                if (stats) { stats->ms_setup += ms_a[0]; stats->ms_search += ms_a[1]; }
                 pts_cap = npts + npts / 4 + 1024;
                 if (in->verbose) fprintf(stderr, "pfg: point buffer -> %llu\n", pts_cap);
                 goto restart_search;
             }
             // ---- output ----
-            unsigned *dcount, *dfill, *didx, *dpad; unsigned long long *dseg; int64_t *dkeys;
+            unsigned *dcount, *dfill, *didx, *dperm, *dperm2, *dsidx;
+            unsigned long long *dseg, *dcseg, *dsum; int64_t *dkeys;
+            const unsigned long long np1 = std::max<unsigned long long>(npts, 1);
             WS(dcount, W_COUNT, (size_t)nb * 4);
             WS(dfill, W_FILL, (size_t)nb * 4);
             WS(dseg, W_SEG, (size_t)(nb + 1) * 8);
-            WS(didx, W_IDX, std::max<unsigned long long>(npts, 1) * 4);
-            WS(dpad, W_PAD, std::max<unsigned long long>(npts, 1) * 8 + 256);
+            WS(dcseg, W_CSEG, (size_t)(nb + 1) * 8);
+            WS(dsum, W_SUM, 64);
+            WS(didx, W_IDX, np1 * 4);
+            WS(dperm, W_PERM, np1 * 4);
+            WS(dperm2, W_PERM2, np1 * 4);
+            WS(dsidx, W_SIDX, np1 * 4);
             int ks = 3;
             for (int k = 0; k < nb; ++k) ks = std::max(ks, geos[in->pgeo[off + k]].h);
-            WS(dkeys, W_KEYS, std::max<unsigned long long>(npts, 1) * ks * 8);
+            WS(dkeys, W_KEYS, np1 * ks * 8);
             CK(cudaMemset(dcount, 0, (size_t)nb * 4));
             CK(cudaMemset(dfill, 0, (size_t)nb * 4));
             CK(cudaEventRecord(ev[3]));
-            OutArgs O{ddirs, dslab, dhdr, dcoords, ddirpass, npts, nb, dcount, dfill, dseg, didx, dkeys, ks, dpad};
+            OutArgs O{ddirs, dslab, dhdr, dcoords, ddirpass, npts, nb, dcount, dfill, dseg, didx, dkeys, ks,
+                      dcseg, dsum, dperm};
             if (npts) { k_count<<<nsm * 4, 256>>>(O); ++launches; }
             k_scan<<<1, 1024>>>(O); ++launches;
             if (npts) { k_scatter<<<nsm * 4, 256>>>(O); ++launches; }
             CK(cudaGetLastError());
-            unsigned long long n_out = 0;
-            CK(cudaMemcpy(&n_out, dseg + nb, 8, cudaMemcpyDeviceToHost));
+            unsigned long long summary[3] = {0, 0, 0};
+            CK(cudaMemcpy(summary, dsum, sizeof summary, cudaMemcpyDeviceToHost));
+            const unsigned long long n_out = summary[0], n_chunks = summary[1], longest = summary[2];
             int64_t *oM, *oK, *oq, *op;
             WS(oM, W_OM, std::max<unsigned long long>(n_out, 1) * MH * 8);
             WS(oK, W_OK, std::max<unsigned long long>(n_out, 1) * MH * 8);
@@ -485,8 +500,15 @@ extern "C" int pfg_coni_batch_ex(const pfg_input *in, const pfg_options *opt_in,
                 const int smem_sort = SORT_CAP * KEYN * 8 + SORT_CAP * 4;
                 CK(cudaFuncSetAttribute(k_segsort, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_sort));
                 k_keys<<<nsm * 4, 256>>>(O, n_out); ++launches;
-                k_segsort<<<std::min(nb, nsm * 3), 256, smem_sort>>>(O); ++launches;
-                RowArgs R{ddirs, dslab, dhdr, dcoords, didx, n_out, off, oM, oK, oq, op};
+                k_segsort<<<(int)std::min<unsigned long long>(n_chunks, (unsigned long long)nsm * 3), 256,
+                            smem_sort>>>(O); ++launches;
+                unsigned *pin = dperm, *pout = dperm2;
+                for (unsigned long long L = SORT_CAP; L < longest; L *= 2) {
+                    k_merge<<<nsm * 8, 256>>>(O, n_out, (unsigned)L, pin, pout); ++launches;
+                    std::swap(pin, pout);
+                }
+                k_order<<<nsm * 4, 256>>>(O, n_out, pin, dsidx); ++launches;
+                RowArgs R{ddirs, dslab, dhdr, dcoords, dsidx, n_out, off, oM, oK, oq, op};
                 k_rows<<<nsm * 8, 256>>>(R); ++launches;
                 CK(cudaGetLastError());
             }

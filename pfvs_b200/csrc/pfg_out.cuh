@@ -5,13 +5,17 @@
 // host, pfvs/fp_kernel/cuda/pfvs_gpu.cu:672-699).  All on the device:
 //   k_count    kept points per direction (the direction succeeded, and the
 //              point comes from the direction's last search pass)
-//   k_scan     segment offsets (one block)
+//   k_scan     segment offsets, sort-chunk offsets, longest segment (one block)
 //   k_scatter  point indices into their direction's segment
 //   k_keys     per kept point its M row (h entries, stride ks): the sort key
 //              (c -> M = Binter c is injective, so M alone orders the points)
-//   k_segsort  one block per segment: bitonic sort of the segment by M; up
-//              to SORT_CAP points in shared memory with the first KEYN
-//              entries of M there, ties on them decided from the full row
+//   k_segsort  one block per chunk (a segment's points in runs of SORT_CAP):
+//              bitonic sort in shared memory on the first KEYN entries of M,
+//              ties decided from the full row
+//   k_merge    merges pairs of sorted runs of the longer segments, one
+//              thread per point: its place is its rank in its own run plus
+//              its rank in the partner run (binary search); log2 passes
+//   k_order    the sorted positions -> point indices
 //   k_rows     the MH-wide M and Kn rows, q and pidx in output order
 //
 // The rows are exact in int64: the setup guarantees |Binter|, |Z Binter| <
@@ -23,7 +27,10 @@
 namespace pfg {
 
 constexpr int KEYN = 4;           // M entries in a sort key
-constexpr int SORT_CAP = 2048;    // segment size sorted in shared memory
+#ifndef PFG_SORT_CAP
+#define PFG_SORT_CAP 2048
+#endif
+constexpr int SORT_CAP = PFG_SORT_CAP;   // run length sorted in shared memory
 
 struct OutArgs {
     const Dir *dirs;
@@ -38,7 +45,9 @@ struct OutArgs {
     unsigned *idx;                // (n_kept) point indices, segment-ordered (then sorted)
     int64_t *keys;                // (n_kept, ks) M rows
     int ks;                       // key stride: the largest h11 of the batch
-    unsigned *pad;                // (2 n_kept + 64) scratch of the long segments
+    unsigned long long *cseg;     // (n_dirs + 1) sort-chunk offsets
+    unsigned long long *summary;  // [0] kept points, [1] chunks, [2] longest segment
+    unsigned *perm;               // (n_kept) segment-local positions in sorted order
 };
 
 __device__ __forceinline__ bool dir_ok(int st) { return st == ST_PENDING || st == ST_OK; }
@@ -56,25 +65,45 @@ __global__ void k_count(OutArgs O)
         if (keep_point(O, k)) atomicAdd(&O.count[O.hdr[k].pid], 1u);
 }
 
-// exclusive scan of count[0..n) into seg[0..n] (one block, <= 1024 threads)
-__global__ void k_scan(OutArgs O)
+// exclusive scans of count[0..n) into seg[0..n] and of the chunk counts
+// ceil(count / SORT_CAP) into cseg[0..n]; the longest segment (one block of
+// 1024 threads)
+__global__ void __launch_bounds__(1024) k_scan(OutArgs O)
 {
-    __shared__ unsigned long long part[1024];
+    __shared__ unsigned long long part[1024], cpart[1024];
+    __shared__ unsigned mx[1024];
     const int t = threadIdx.x, nt = blockDim.x, n = O.n_dirs;
     const int per = (n + nt - 1) / nt, a = t * per, b = min(a + per, n);
-    unsigned long long s = 0;
-    for (int i = a; i < b; ++i) s += O.count[i];
-    part[t] = s;
+    unsigned long long s = 0, cs = 0;
+    unsigned m = 0;
+    for (int i = a; i < b; ++i) {
+        const unsigned c = O.count[i];
+        s += c;
+        cs += (c + SORT_CAP - 1) / SORT_CAP;
+        m = max(m, c);
+    }
+    part[t] = s; cpart[t] = cs; mx[t] = m;
     __syncthreads();
     for (int o = 1; o < nt; o <<= 1) {
-        unsigned long long x = t >= o ? part[t - o] : 0;
+        const unsigned long long x = t >= o ? part[t - o] : 0, y = t >= o ? cpart[t - o] : 0;
+        const unsigned z = t >= o ? mx[t - o] : 0;
         __syncthreads();
-        part[t] += x;
+        part[t] += x; cpart[t] += y; mx[t] = max(mx[t], z);
         __syncthreads();
     }
-    unsigned long long run = t ? part[t - 1] : 0;
-    for (int i = a; i < b; ++i) { O.seg[i] = run; run += O.count[i]; }
-    if (t == nt - 1) O.seg[n] = part[nt - 1];
+    unsigned long long run = t ? part[t - 1] : 0, crun = t ? cpart[t - 1] : 0;
+    for (int i = a; i < b; ++i) {
+        const unsigned c = O.count[i];
+        O.seg[i] = run; run += c;
+        O.cseg[i] = crun; crun += (c + SORT_CAP - 1) / SORT_CAP;
+    }
+    if (t == nt - 1) {
+        O.seg[n] = part[nt - 1];
+        O.cseg[n] = cpart[nt - 1];
+        O.summary[0] = part[nt - 1];
+        O.summary[1] = cpart[nt - 1];
+        O.summary[2] = mx[nt - 1];
+    }
 }
 
 __global__ void k_scatter(OutArgs O)
@@ -124,12 +153,19 @@ __device__ __forceinline__ bool key_greater(const OutArgs &O, const int64_t *pre
     return x > y;                                   // (equal rows: the same point)
 }
 
-// One block per direction: bitonic sort of the segment's local positions by
-// M, padded to a power of two with sentinels.  Segments up to SORT_CAP points
-// sort in shared memory (with the first KEYN entries of each M row copied
-// in); longer ones in the scratch region pad[2 s0, 2 s0 + np) with the rows
-// read from global memory (np < 2 n, so the regions of different segments
-// are disjoint).
+// x < y for segment-local positions of one segment (rows from global memory)
+__device__ __forceinline__ bool key_less(const OutArgs &O, unsigned long long s0, unsigned x, unsigned y, int h)
+{
+    const int64_t *kx = O.keys + (s0 + x) * O.ks, *ky = O.keys + (s0 + y) * O.ks;
+    for (int r = 0; r < h; ++r)
+        if (kx[r] != ky[r]) return kx[r] < ky[r];
+    return x < y;
+}
+
+// One block per chunk: bitonic sort (padded to a power of two with
+// sentinels) of SORT_CAP or fewer consecutive points of one segment, the
+// first KEYN entries of their M rows in shared memory.  Writes the chunk's
+// segment-local positions in sorted order to perm.
 __global__ void __launch_bounds__(256) k_segsort(OutArgs O)
 {
 #ifdef PFG_EMU
@@ -138,22 +174,27 @@ __global__ void __launch_bounds__(256) k_segsort(OutArgs O)
     extern __shared__ __align__(16) unsigned char smem_raw[];
 #endif
     int64_t *skeys = (int64_t *)smem_raw;                       // SORT_CAP x KEYN
-    unsigned *sperm = (unsigned *)(skeys + SORT_CAP * KEYN);    // SORT_CAP
+    unsigned *a = (unsigned *)(skeys + SORT_CAP * KEYN);        // SORT_CAP
     constexpr unsigned NONE = 0xffffffffu;
-    for (int pid = blockIdx.x; pid < O.n_dirs; pid += gridDim.x) {
+    const unsigned long long nch = O.summary[1];
+    for (unsigned long long ci = blockIdx.x; ci < nch; ci += gridDim.x) {
+        int lo_p = 0, hi_p = O.n_dirs;              // the direction: cseg[pid] <= ci < cseg[pid + 1]
+        while (hi_p - lo_p > 1) {
+            const int mid = (lo_p + hi_p) >> 1;
+            if (O.cseg[mid] <= ci) lo_p = mid; else hi_p = mid;
+        }
+        const int pid = lo_p;
         const unsigned long long s0 = O.seg[pid];
-        const unsigned n = (unsigned)(O.seg[pid + 1] - s0);
-        if (n < 2) continue;
-        const Dir D = O.dirs[pid];
+        const unsigned nseg = (unsigned)(O.seg[pid + 1] - s0);
+        const unsigned lo = (unsigned)(ci - O.cseg[pid]) * SORT_CAP;
+        const unsigned n = min((unsigned)SORT_CAP, nseg - lo);
+        const int h = O.dirs[pid].h;
         unsigned np = 1;
         while (np < n) np <<= 1;
-        const bool in_smem = np <= (unsigned)SORT_CAP;
-        unsigned *a = in_smem ? sperm : O.pad + 2 * s0;
-        if (in_smem)
-            for (unsigned e = threadIdx.x; e < n * KEYN; e += blockDim.x) {
-                const unsigned t = e / KEYN, r = e % KEYN;
-                skeys[e] = (int)r < D.h ? O.keys[(s0 + t) * O.ks + r] : 0;
-            }
+        for (unsigned e = threadIdx.x; e < n * KEYN; e += blockDim.x) {
+            const unsigned t = e / KEYN, r = e % KEYN;
+            skeys[e] = (int)r < h ? O.keys[(s0 + lo + t) * O.ks + r] : 0;
+        }
         for (unsigned t = threadIdx.x; t < np; t += blockDim.x) a[t] = t < n ? t : NONE;
         __syncthreads();
         for (unsigned k = 2; k <= np; k <<= 1) {
@@ -166,23 +207,49 @@ __global__ void __launch_bounds__(256) k_segsort(OutArgs O)
                     bool xgt;                       // x > y
                     if (x == NONE) xgt = y != NONE;
                     else if (y == NONE) xgt = false;
-                    else if (in_smem) xgt = key_greater(O, skeys, s0, x, y, D.h);
-                    else {                          // long segment: whole rows from global memory
-                        const int64_t *kx = O.keys + (s0 + x) * O.ks, *ky = O.keys + (s0 + y) * O.ks;
-                        int r = 0;
-                        while (r < D.h && kx[r] == ky[r]) ++r;
-                        xgt = r < D.h ? kx[r] > ky[r] : x > y;
-                    }
+                    else xgt = key_greater(O, skeys, s0 + lo, x, y, h);
                     if (xgt == up) { a[t] = y; a[u] = x; }
                 }
                 __syncthreads();
             }
         }
-        // a holds the local positions in sorted order: map them to point indices in place
-        for (unsigned t = threadIdx.x; t < n; t += blockDim.x) a[t] = O.idx[s0 + a[t]];
+        for (unsigned t = threadIdx.x; t < n; t += blockDim.x) O.perm[s0 + lo + t] = lo + a[t];
         __syncthreads();
-        for (unsigned t = threadIdx.x; t < n; t += blockDim.x) O.idx[s0 + t] = a[t];
-        __syncthreads();
+    }
+}
+
+// One merge pass over runs of length L (segments longer than L only): the
+// point at segment position i of run r goes to the merged run of runs
+// (r & ~1, r | 1) at its rank in its own run plus its rank in the partner.
+__global__ void k_merge(OutArgs O, unsigned long long n_kept, unsigned L, const unsigned *pin, unsigned *pout)
+{
+    for (unsigned long long t = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; t < n_kept;
+         t += (unsigned long long)gridDim.x * blockDim.x) {
+        const int pid = O.hdr[O.idx[t]].pid;
+        const unsigned long long s0 = O.seg[pid];
+        const unsigned n = (unsigned)(O.seg[pid + 1] - s0), i = (unsigned)(t - s0);
+        if (n <= L) { pout[t] = pin[t]; continue; }
+        const unsigned r = i / L, own_lo = r * L, part_lo = (r ^ 1u) * L, base = (r & ~1u) * L;
+        const unsigned part_n = part_lo >= n ? 0 : min(L, n - part_lo);
+        const unsigned x = pin[t];
+        const int h = O.dirs[pid].h;
+        unsigned lo = 0, hi = part_n;               // partner elements less than x
+        while (lo < hi) {
+            const unsigned mid = (lo + hi) >> 1;
+            if (key_less(O, s0, pin[s0 + part_lo + mid], x, h)) lo = mid + 1; else hi = mid;
+        }
+        pout[s0 + base + (i - own_lo) + lo] = x;
+    }
+}
+
+// sorted segment-local positions -> point indices in output order
+__global__ void k_order(OutArgs O, unsigned long long n_kept, const unsigned *perm, unsigned *out_idx)
+{
+    for (unsigned long long t = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; t < n_kept;
+         t += (unsigned long long)gridDim.x * blockDim.x) {
+        const int pid = O.hdr[O.idx[t]].pid;
+        const unsigned long long s0 = O.seg[pid];
+        out_idx[t] = O.idx[s0 + perm[t]];
     }
 }
 

@@ -19,8 +19,10 @@ def build():
     os.makedirs(os.path.dirname(LIB), exist_ok=True)
     if os.path.exists(LIB) and all(os.path.getmtime(s) <= os.path.getmtime(LIB) for s in SRCS):
         return
+    # -DPFG_SORT_CAP=1: the output sort starts from runs of one point here, so that
+    # every direction with 2 or more points goes through the run-merge passes
     subprocess.run(["g++", "-std=c++20", "-O1", "-g", "-pthread", "-shared", "-fPIC", "-w",
-                    os.path.join(HERE, "emu_driver.cpp"), "-o", LIB], check=True)
+                    "-DPFG_SORT_CAP=1", os.path.join(HERE, "emu_driver.cpp"), "-o", LIB], check=True)
 
 
 def _load():

@@ -105,18 +105,19 @@ extern "C" int emu_coni_batch(const pfg_input *in, int precision, int n_warps, p
     if (ctl[0].err || ctl[1].err) { snprintf(out->err, sizeof out->err, "wait ran out"); return 1; }
     const unsigned long long npts = ctl[0].npts;
     if (npts > pts_cap) { snprintf(out->err, sizeof out->err, "point buffer overflow"); return 1; }
-    std::vector<unsigned> cnt(nb, 0), fill(nb, 0), idx(std::max<unsigned long long>(npts, 1)),
-        pad(2 * std::max<unsigned long long>(npts, 1) + 64);
+    const unsigned long long np1 = std::max<unsigned long long>(npts, 1);
+    std::vector<unsigned> cnt(nb, 0), fill(nb, 0), idx(np1), perm(np1), perm2(np1), sidx(np1);
     int ks = 3;
     for (int k = 0; k < nb; ++k) ks = std::max(ks, geos[pgeo[k]].h);
-    std::vector<int64_t> keys(std::max<unsigned long long>(npts, 1) * ks);
-    std::vector<unsigned long long> seg(nb + 1, 0);
+    std::vector<int64_t> keys(np1 * ks);
+    std::vector<unsigned long long> seg(nb + 1, 0), cseg(nb + 1, 0), summary(4, 0);
     OutArgs O{dirs.data(), slab.data(), hdr.data(), coords.data(), dpass.data(), npts, nb,
-              cnt.data(), fill.data(), seg.data(), idx.data(), keys.data(), ks, pad.data()};
+              cnt.data(), fill.data(), seg.data(), idx.data(), keys.data(), ks, cseg.data(), summary.data(),
+              perm.data()};
     if (npts) launch(4, [&] { k_count(O); });
     launch(1, [&] { k_scan(O); });
     if (npts) launch(4, [&] { k_scatter(O); });
-    const unsigned long long n_out = seg[nb];
+    const unsigned long long n_out = summary[0], n_chunks = summary[1], longest = summary[2];
     out->n = (int64_t)n_out;
     out->M = (int64_t *)malloc(n_out * MH * 8 + 8);
     out->Kn = (int64_t *)malloc(n_out * MH * 8 + 8);
@@ -124,8 +125,14 @@ extern "C" int emu_coni_batch(const pfg_input *in, int precision, int n_warps, p
     out->pidx = (int64_t *)malloc(n_out * 8 + 8);
     if (n_out) {
         launch(4, [&] { k_keys(O, n_out); });
-        launch(std::min(nb, 8), [&] { k_segsort(O); });
-        RowArgs R{dirs.data(), slab.data(), hdr.data(), coords.data(), idx.data(), n_out, 0,
+        launch((unsigned)std::min<unsigned long long>(n_chunks, 8), [&] { k_segsort(O); });
+        unsigned *pin = perm.data(), *pout = perm2.data();
+        for (unsigned long long L = SORT_CAP; L < longest; L *= 2) {
+            launch(4, [&] { k_merge(O, n_out, (unsigned)L, pin, pout); });
+            std::swap(pin, pout);
+        }
+        launch(4, [&] { k_order(O, n_out, pin, sidx.data()); });
+        RowArgs R{dirs.data(), slab.data(), hdr.data(), coords.data(), sidx.data(), n_out, 0,
                   out->M, out->Kn, out->q, out->pidx};
         launch(4, [&] { k_rows(R); });
     }

@@ -8,7 +8,8 @@
 // atomics map to GCC __atomic builtins.  Warps of a grid run one after
 // another (the kernels' cross-warp protocols stay correct, only serial).
 #pragma once
-#include <barrier>
+#include <atomic>
+#include <sched.h>
 #include <chrono>
 #include <cmath>
 #include <cstdint>
@@ -27,8 +28,25 @@
 
 struct dim3 { unsigned x = 1, y = 1, z = 1; };
 
+// Barrier of the 32 lane threads: spin with yield (lanes meet at every
+// collective, far too often for a sleeping barrier to keep up).
+struct EmuBarrier {
+    std::atomic<int> count{0};
+    std::atomic<unsigned> phase{0};
+    void arrive_and_wait()
+    {
+        const unsigned ph = phase.load(std::memory_order_acquire);
+        if (count.fetch_add(1, std::memory_order_acq_rel) == 31) {
+            count.store(0, std::memory_order_relaxed);
+            phase.fetch_add(1, std::memory_order_acq_rel);
+        } else {
+            while (phase.load(std::memory_order_acquire) == ph) sched_yield();
+        }
+    }
+};
+
 struct EmuWarp {
-    std::barrier<> bar{32};
+    EmuBarrier bar;
     unsigned char slot[32][16];
     int site[32];
     int hist[32][64];

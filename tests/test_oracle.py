@@ -167,10 +167,20 @@ def test_device_code_under_warp_emulator():
     """The library's device sources, run on CPU threads (tests/emu), equal the
     oracle on a small case; divergent warp collectives abort the run."""
     from emu import emu
+    # plain h11 = 11 at dilation 150: three directions with points (one with two)
     w = workloads.build("plain", n_p=96, dilations=(150.0,))
     geoms, ps, pgeo, _ = layout(w)
-    sel = [3, 25, 65, 86]                   # three of them emit points, one emits two
+    sel = [3, 25, 65, 86]
     ps, pgeo = [ps[i] for i in sel], pgeo[sel]
     M, Kn, q, pidx, pstat, nodes, stage = emu.coni_batch_multi(geoms, ps, pgeo)
     assert np.all(pstat == 0) and nodes.sum() > 0 and len(q) == 4
     assert_same((M, Kn, q, pidx), expected(geoms, ps, pgeo, "oracle"))
+    # mixed h11 = 8 .. 32: directions of the h11 = 32 geometry with 3 and 47 points
+    # (the emulator build sorts from runs of one point, so these go through the merges)
+    w = workloads.build("mixed", n_p=96)
+    geoms, ps, pgeo, _ = layout(w)
+    sel = [3, 83, 85, 87]
+    ps, pgeo = [ps[i] for i in sel], pgeo[sel]
+    got = emu.coni_batch_multi(geoms, ps, pgeo)
+    assert np.all(got[4] == 0) and len(got[2]) == 51
+    assert_same(got[:4], expected(geoms, ps, pgeo, "oracle"))
