@@ -206,6 +206,13 @@ extern "C" int pfg_debug_stage_cycles(unsigned long long *out)
     unsigned long long z[64] = {};
     return cudaMemcpyToSymbol(pfg::pfg_stage_cycles, z, sizeof z) != cudaSuccess;
 }
+// profiling build only: the search's busy / waiting cycles and subtree counts (and zero them)
+extern "C" int pfg_debug_search_cycles(unsigned long long *out)
+{
+    if (cudaMemcpyFromSymbol(out, pfg::pfg_search_cycles, sizeof(unsigned long long) * 8) != cudaSuccess) return 1;
+    unsigned long long z[8] = {};
+    return cudaMemcpyToSymbol(pfg::pfg_search_cycles, z, sizeof z) != cudaSuccess;
+}
 #endif
 extern "C" const char *pfg_backend(void) { return "cuda"; }
 
@@ -407,39 +414,64 @@ extern "C" int pfg_coni_batch_ex(const pfg_input *in, const pfg_options *opt_in,
                 A.dir_nodes = ddirnodes; A.eps = 1e-4; A.wait_ns = 30ll * 1000000000ll;
                 A.npts = &dctl->npts;
                 A.deadline_ns = 120ll * 1000000000ll;
-                const int wpb = opt.warps_per_block > 0 ? opt.warps_per_block : 8;
+                // per-warp staging area in shared memory, sized for the batch's largest h11
+                int hmax = 3;
+                for (int k = 0; k < nb; ++k) hmax = std::max(hmax, geos[in->pgeo[off + k]].h);
+                const unsigned st32 = stage_bytes<float>(hmax - 1, hmax), st64 = stage_bytes<double>(hmax - 1, hmax);
+                const int smem_max = 227 * 1024;
+                auto warps_for = [&](unsigned st) {
+                    const int w = opt.warps_per_block > 0 ? opt.warps_per_block : 8;
+                    return std::max(1, std::min(w, smem_max / (int)st));
+                };
+                const int wpb32 = warps_for(st32), wpb64 = warps_for(st64);
+                CK(cudaFuncSetAttribute(k_search<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, wpb32 * st32));
+                CK(cudaFuncSetAttribute(k_search<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, wpb64 * st64));
                 if (opt.form == PFG_FORM_PLAIN) {
+                    CK(cudaFuncSetAttribute(k_search_plain<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, st32));
+                    CK(cudaFuncSetAttribute(k_search_plain<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, st64));
                     A.donate = 0; A.n_warps = 1;
                     A.ctl = dctl;
+                    A.stage_bytes = st32;
                     for (int k = 0; k < nb; ++k) {
                         const bool f32 = geos[in->pgeo[off + k]].use_f32;
-                        if (f32) { k_search_plain<float><<<1, 32>>>(A, k); ++launches; }
+                        if (f32) { k_search_plain<float><<<1, 32, st32>>>(A, k); ++launches; }
                     }
                     k_flip<<<(nb + 255) / 256, 256>>>(ddirs, dgeo, nb, 1, ddirpass, dretry); ++launches;
                     A.pass = 2;
-                    for (int k = 0; k < nb; ++k) { k_search_plain<double><<<1, 32>>>(A, k); ++launches; }
+                    A.stage_bytes = st64;
+                    for (int k = 0; k < nb; ++k) { k_search_plain<double><<<1, 32, st64>>>(A, k); ++launches; }
                     CK(cudaGetLastError());
                 } else {
-                    int bps = opt.blocks_per_sm;
-                    if (bps <= 0) {
-                        int mb32 = 0;
-                        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&mb32, k_search<float>, wpb * 32, 0));
-                        bps = std::max(1, mb32);
-                    }
-                    const int grid = nsm * bps;
-                    A.donate = 1; A.n_warps = grid * wpb;
+                    auto grid_for = [&](const void *fn, int wpb, unsigned st, int &grid) -> cudaError_t {
+                        int bps = opt.blocks_per_sm;
+                        if (bps <= 0) {
+                            cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, fn, wpb * 32,
+                                                                                          (size_t)wpb * st);
+                            if (e != cudaSuccess) return e;
+                            bps = std::max(1, bps);
+                        }
+                        grid = nsm * bps;
+                        return cudaSuccess;
+                    };
+                    A.donate = 1;
                     // FP32 pass over the FP32 geometries' directions
                     if (!todo32.empty()) {
+                        int grid = 0;
+                        CK(grid_for((const void *)k_search<float>, wpb32, st32, grid));
+                        A.n_warps = grid * wpb32; A.stage_bytes = st32;
                         A.ctl = dctl; A.todo = dtodo32; A.n_todo = (int)todo32.size(); A.pass = 1;
                         CK(cudaMemset(dready, 0, (size_t)q_cap * 4));
-                        k_search<float><<<grid, wpb * 32>>>(A); ++launches;
+                        k_search<float><<<grid, wpb32 * 32, (size_t)wpb32 * st32>>>(A); ++launches;
                         CK(cudaGetLastError());
                     }
                     k_flip<<<(nb + 255) / 256, 256>>>(ddirs, dgeo, nb, 1, ddirpass, dretry); ++launches;
                     // FP64 pass over everything still pending
+                    int grid = 0;
+                    CK(grid_for((const void *)k_search<double>, wpb64, st64, grid));
+                    A.n_warps = grid * wpb64; A.stage_bytes = st64;
                     A.ctl = dctl + 1; A.todo = dtodoall; A.n_todo = nb; A.pass = 2;
                     CK(cudaMemset(dready, 0, (size_t)q_cap * 4));
-                    k_search<double><<<grid, wpb * 32>>>(A); ++launches;
+                    k_search<double><<<grid, wpb64 * 32, (size_t)wpb64 * st64>>>(A); ++launches;
                     CK(cudaGetLastError());
                 }
             }

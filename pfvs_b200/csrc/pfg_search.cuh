@@ -66,6 +66,7 @@ struct SearchArgs {
     int n_warps;                  // warps of the persistent grid
     long long wait_ns;            // bound on idle waiting (globaltimer ns)
     long long deadline_ns;        // bound on one subtree's search (globaltimer ns)
+    unsigned stage_bytes;         // per-warp staging area (dynamic shared memory), stage_bytes<R>(d max)
 };
 
 __device__ __forceinline__ unsigned long long gtimer()
@@ -118,27 +119,57 @@ template <> struct Num<double> {
     static __device__ double i32max() { return 2147483647.0; }
 };
 
+// The search data of one direction, staged by the warp that searches it:
+// U packed by rows (upper triangle, row i holds U[i][i..d-1]), 1/U_ii, and
+// mat and ZB^T as int32 (the setup bounds their entries by 2^25); the
+// GCD-cut rows H stay in global memory (only large trees have them).
+PFG_HD int upk(int i, int j, int d) { return i * d - ((i * (i - 1)) >> 1) + (j - i); }
+template <class R> PFG_HD unsigned stage_bytes(int d, int h)
+{
+    unsigned b = (unsigned)((d * (d + 1) / 2 + d) * sizeof(R));
+    b = (b + 15u) & ~15u;
+    b += (unsigned)(d * d + d * h) * 4u;
+    return (b + 15u) & ~15u;
+}
+
 template <class R> struct Prob {
-    const R *U, *UI;
-    const int64_t *H, *MAT, *BT, *ZT;
+    const R *U, *UI;                  // staged: U packed (upk), 1/U_ii
+    const int32_t *MAT, *ZT;          // staged: mat (d x d), ZT (d x h)
+    const int64_t *H;                 // global
     int d, h, m0_level, pad;
     int64_t g_lin, Q, qmax, linmin;
     uint64_t hrows;
     R qmax_r, slack, Kerr, max_err;
 };
 
-template <class R> __device__ Prob<R> load_prob(const SearchArgs &A, int pid)
+// Set up the problem of direction pid and stage its data in `stage` (the
+// warp's area: shared memory in the batched kernels).  Warp-collective.
+template <class R> __device__ Prob<R> load_prob(const SearchArgs &A, int pid, void *stage, int lane)
 {
     const Dir D = A.dirs[pid];
     const Geo g = A.geo[D.geo];
-    const Slab L = slab_layout(D.h, D.d);
+    const int d = D.d, h = D.h;
+    const Slab L = slab_layout(h, d);
     const int64_t *s = A.slab + D.slab;
+    const R *Ug = sizeof(R) == 4 ? (const R *)(s + L.u32) : (const R *)(s + L.u64);
+    const R *UIg = sizeof(R) == 4 ? (const R *)(s + L.ui32) : (const R *)(s + L.ui64);
+    const int64_t *MATg = s + L.mat, *ZTg = s + L.zt;
+    R *U = (R *)stage, *UI = U + d * (d + 1) / 2;
+    int32_t *MAT = (int32_t *)((char *)stage + ((((d * (d + 1) / 2 + d) * sizeof(R)) + 15) & ~(size_t)15));
+    int32_t *ZT = MAT + d * d;
+    __syncwarp();                                   // (the previous problem's readers are done)
+    for (int e = lane; e < d * d; e += 32) {
+        const int i = e / d, j = e - i * d;
+        if (j >= i) U[upk(i, j, d)] = Ug[e];
+        MAT[e] = (int32_t)MATg[e];
+    }
+    for (int e = lane; e < d; e += 32) UI[e] = UIg[e];
+    for (int e = lane; e < d * h; e += 32) ZT[e] = (int32_t)ZTg[e];
+    __syncwarp();
     Prob<R> P;
-    P.d = D.d; P.h = D.h; P.m0_level = D.m0_level;
+    P.d = d; P.h = h; P.m0_level = D.m0_level;
     P.g_lin = D.g_lin; P.Q = g.Q; P.qmax = g.qmax; P.linmin = g.linmin; P.hrows = D.hrows;
-    if (sizeof(R) == 4) { P.U = (const R *)(s + L.u32); P.UI = (const R *)(s + L.ui32); }
-    else { P.U = (const R *)(s + L.u64); P.UI = (const R *)(s + L.ui64); }
-    P.H = s + L.H; P.MAT = s + L.mat; P.BT = s + L.bt; P.ZT = s + L.zt;
+    P.U = U; P.UI = UI; P.MAT = MAT; P.ZT = ZT; P.H = s + L.H;
     const R qd = (R)g.qmax;
     P.qmax_r = qd;
     // search constants (fpk_search_impl.h:30-39), plus the certified margin
@@ -189,10 +220,10 @@ template <class R> __device__ __forceinline__ void apply_dc(Lanes<R> &S, const P
 {
     if (dv == 0 || i == 0) return;
     const int d = P.d, h = P.h;
-    if (lane < d) S.y0 += P.MAT[i * d + lane] * dv;
-    if (lane + 32 < d) S.y1 += P.MAT[i * d + lane + 32] * dv;
-    if (lane < h) S.k0 += P.ZT[i * h + lane] * dv;
-    if (lane + 32 < h) S.k1 += P.ZT[i * h + lane + 32] * dv;
+    if (lane < d) S.y0 += (int64_t)P.MAT[i * d + lane] * dv;
+    if (lane + 32 < d) S.y1 += (int64_t)P.MAT[i * d + lane + 32] * dv;
+    if (lane < h) S.k0 += (int64_t)P.ZT[i * h + lane] * dv;
+    if (lane + 32 < h) S.k1 += (int64_t)P.ZT[i * h + lane + 32] * dv;
 }
 
 // the dot products of entering level i (c[i+1:] set): off, aoff, GCD prefix
@@ -203,15 +234,16 @@ template <class R> __device__ __forceinline__ void level_sums(const Lanes<R> &S,
     R o = 0, a = 0;
     i128 pr = 0;
     const bool hrow = (P.hrows >> i) & 1;
+    const R *Ui = P.U + upk(i, i, d) - i;           // Ui[j] = U[i][j], j >= i
     int j = lane;
     if (j > i && j < d) {
-        R t = P.U[i * d + j] * (R)S.c0;
+        R t = Ui[j] * (R)S.c0;
         o += t; a += fabs(t);
         if (hrow) pr += (i128)P.H[i * d + j] * S.c0;
     }
     j = lane + 32;
     if (j > i && j < d) {
-        R t = P.U[i * d + j] * (R)S.c1;
+        R t = Ui[j] * (R)S.c1;
         o += t; a += fabs(t);
         if (hrow) pr += (i128)P.H[i * d + j] * S.c1;
     }
@@ -320,7 +352,7 @@ __device__ int run_subtree(const SearchArgs &A, const Prob<R> &P, int pid, const
     i128 A0 = 0;
     int64_t B0 = 0;
     if (i == 0) leaf_data(S, P, lane, A0, B0);
-    const int64_t m00 = P.MAT[0];
+    const int64_t m00 = (int64_t)P.MAT[0];
     unsigned poll = 0;
     const unsigned long long t0 = shfl(gtimer(), 0);
     for (;;) {
@@ -378,7 +410,7 @@ __device__ int run_subtree(const SearchArgs &A, const Prob<R> &P, int pid, const
         const i128 pre = shfl128(i < 32 ? S.pre0 : S.pre1, i & 31);
         const bool hrow = (P.hrows >> i) & 1;
         const int64_t hii = hrow ? P.H[i * d + i] : 0;
-        const R uii = P.U[i * d + i];
+        const R uii = P.U[upk(i, i, d)];
         const int64_t ncand = min((int64_t)32, hi - cur + 1);
         const int64_t v = cur + lane;
         bool pass = lane < ncand;
@@ -449,8 +481,8 @@ __device__ int run_subtree(const SearchArgs &A, const Prob<R> &P, int pid, const
             const int64_t vt = cur + t;
             const i128 qt = shfl128(q, t);
             uint64_t g = 0;
-            if (lane >= 1 && lane < h) g = gcd64(g, uabs64(S.k0 + P.ZT[lane] * vt));
-            if (lane + 32 < h) g = gcd64(g, uabs64(S.k1 + P.ZT[lane + 32] * vt));
+            if (lane >= 1 && lane < h) g = gcd64(g, uabs64(S.k0 + (int64_t)P.ZT[lane] * vt));
+            if (lane + 32 < h) g = gcd64(g, uabs64(S.k1 + (int64_t)P.ZT[lane + 32] * vt));
             for (int o = 16; o; o >>= 1) g = gcd64(g, __shfl_xor_sync(FULL, g, o));
             if (g != 0 && (i128)P.Q * (i128)g <= qt && lane == t) ok = false;
         }
@@ -496,13 +528,37 @@ __device__ void finish_item(const SearchArgs &A, int pid, int st, Tally &T, int 
 
 // Persistent batched search: warps take directions from the todo list, then
 // donated nodes from the queue; all bounded waits report ST_WAIT.
+#ifdef PFG_EMU
+static unsigned char emu_stage[64 * 1024];
+#define PFG_STAGE_AREA(A) ((void *)emu_stage)
+#else
+#define PFG_STAGE_AREA(A) ((void *)(pfg_stage_smem + (threadIdx.x >> 5) * (A).stage_bytes))
+#endif
+
+// Profiling build only (-DPFG_STAGE_CLOCKS): per pass (float 0, double 1)
+// the warps' clock64() cycles spent searching [0/1] and waiting for work
+// [2/3], and the subtrees run [4/5].
+#ifdef PFG_STAGE_CLOCKS
+__device__ unsigned long long pfg_search_cycles[8];
+#define PFG_SCLK(v) long long v = clock64()
+#define PFG_SADD(i, x) do { if (lane == 0) atomicAdd(&pfg_search_cycles[(i) + (sizeof(R) == 8)], (unsigned long long)(x)); } while (0)
+#else
+#define PFG_SCLK(v) do { } while (0)
+#define PFG_SADD(i, x) do { } while (0)
+#endif
+
 template <class R>
-__global__ void __launch_bounds__(256) k_search(SearchArgs A)
+__global__ void __launch_bounds__(256, 2) k_search(SearchArgs A)
 {
+#ifndef PFG_EMU
+    extern __shared__ __align__(16) unsigned char pfg_stage_smem[];
+#endif
+    void *stage = PFG_STAGE_AREA(A);
     const int lane = threadIdx.x & 31;
     Tally T{0, 0, 0};
     const unsigned long long t_start = gtimer();
     for (;;) {
+        PFG_SCLK(c_wait);
         int pid = -1;
         const WorkItem *it = nullptr;
         int got = 0;                              // 1 root, 2 queue item
@@ -556,11 +612,18 @@ __global__ void __launch_bounds__(256) k_search(SearchArgs A)
         it = (const WorkItem *)ip;
         int st = 0;
         int pending = 0;
+        PFG_SCLK(c_run);
         if (lane == 0) pending = ((volatile Dir *)A.dirs)[pid].status == ST_PENDING;
         if (shfl(pending, 0)) {                   // (skip work of a direction that already failed)
-            const Prob<R> P = load_prob<R>(A, pid);
+            const Prob<R> P = load_prob<R>(A, pid, stage, lane);
             st = run_subtree<R>(A, P, pid, it, T, lane);
         }
+#ifdef PFG_STAGE_CLOCKS
+        PFG_SCLK(c_end);
+        PFG_SADD(0, c_end - c_run);
+        PFG_SADD(2, c_run - c_wait);
+        PFG_SADD(4, 1);
+#endif
         finish_item<R>(A, pid, st, T, lane);
         __threadfence();
         if (lane == 0) atomicSub(&A.ctl->active, 1);
@@ -571,12 +634,16 @@ __global__ void __launch_bounds__(256) k_search(SearchArgs A)
 template <class R>
 __global__ void __launch_bounds__(32) k_search_plain(SearchArgs A, int pid)
 {
+#ifndef PFG_EMU
+    extern __shared__ __align__(16) unsigned char pfg_stage_smem[];
+#endif
+    void *stage = PFG_STAGE_AREA(A);
     const int lane = threadIdx.x & 31;
     Tally T{0, 0, 0};
     int pending = 0;
     if (lane == 0) pending = A.dirs[pid].status == ST_PENDING;
     if (!shfl(pending, 0)) return;
-    const Prob<R> P = load_prob<R>(A, pid);
+    const Prob<R> P = load_prob<R>(A, pid, stage, lane);
     int st = run_subtree<R>(A, P, pid, nullptr, T, lane);
     finish_item<R>(A, pid, st, T, lane);
 }

@@ -530,7 +530,10 @@ PFG_NOINLINE __device__ int warp_unimodular(const int64_t *vin, int n, int64_t *
 }
 
 #ifndef PFG_DELTA_H
-#define PFG_DELTA_H 0.99
+#define PFG_DELTA_H 0.99        // LLL parameter of the GCD-row reductions
+#endif
+#ifndef PFG_DELTA_O
+#define PFG_DELTA_O 0.99        // LLL parameter of the Euclidean reduction of O
 #endif
 
 // ---------------------------------------------------------------------------
@@ -590,7 +593,7 @@ template <int N> __device__ int setup_one(const SetupArgs &A, int pid, int lane,
     if (gram_euclid<N>(S, d, h, lane)) return ST_OVERFLOW;
     {
         Lll<N> LL{S, h, d};
-        if ((st = warp_lll(LL, d, false, 0.99, lane))) return st;
+        if ((st = warp_lll(LL, d, false, PFG_DELTA_O, lane))) return st;
     }
     clk.mark(5);
     // 5. (Mbasis O^T)^T rows, 6. coni order (rows with entry 0 == 0 first, stable)

@@ -55,6 +55,7 @@ struct StaticScratch {
     int64_t Mrow[STATIC_MAX_POINTS * MH];       // unsorted rows
     int64_t Krow[STATIC_MAX_POINTS * MH];
     unsigned idx[STATIC_MAX_POINTS];
+    unsigned char stage[56 * 1024];             // the search's staging area (stage_bytes<double>(63, 64))
 };
 
 // The scratch.  In host code `g_static` names a host-side stand-in, not the
@@ -109,7 +110,8 @@ __global__ void __launch_bounds__(32) k_direction_static(StaticScratch *S, int h
         A.dir_nodes = S->dir_nodes; A.eps = 1e-4; A.donate = 0; A.n_warps = 1;
         A.wait_ns = 30ll * 1000000000ll; A.deadline_ns = 120ll * 1000000000ll;
         Tally T{0, 0, 0};
-        const Prob<double> P = load_prob<double>(A, 0);
+        static_assert(sizeof(StaticScratch::stage) >= 49664, "staging area");
+        const Prob<double> P = load_prob<double>(A, 0, S->stage, lane);
         st = run_subtree<double>(A, P, 0, nullptr, T, lane);
         npts = shfl(S->ctl.npts, 0);
         if (st == 0 && npts > (unsigned long long)cap) st = -2;   // more points than the caller's buffers
