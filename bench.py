@@ -39,6 +39,24 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
+# Roofline of the dominant kernel (k_setup<32>, the per-direction lattice
+# setup): scalar integer / FP64 warp code, neither HBM- nor tensor-bound, so
+# its ceiling is the warp-instruction issue rate, 148 SMs x 4 schedulers x
+# SM clock.  Per-unit figures from one ncu capture of the kernel on the
+# first 16,384 directions of this batch (profiles/k_setup_mixed.md):
+# executed warp instructions and DRAM bytes per direction.
+SETUP_INST_PER_DIR = 23_323_134_329 / 16384
+SETUP_DRAM_PER_DIR = (64_152_064 + 526_142_464) / 16384
+N_SM, SCHEDULERS = 148, 4
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return json.load(f), "measured"
+    except (OSError, ValueError):
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "sm_max_mhz": 1965.0}, "fallback"
+
 
 def parse():
     ap = argparse.ArgumentParser()
@@ -281,6 +299,9 @@ def main():
     # e2e: the public C ABI (pfg_coni_batch) with host buffers, wall clock
     e2e = None
     if not args.no_e2e:
+        del r
+        out = gpu.coni_batch_multi(geoms, ps, pgeo, device=device)    # (warm-up: pinned output blocks)
+        del out
         barrier(pg)
         t0 = time.perf_counter()
         for _ in range(args.steps):
@@ -308,6 +329,20 @@ def main():
                    "sample": f"{len(pick)} random directions (seed 1) of the batch, "
                              f"{dt:.1f} s on {threads} threads; the reference's own tree nodes",
                    "directions_per_s": rd / dt}
+    # roofline of the setup kernel: executed warp instructions per launch (ncu
+    # per-direction figure x directions) over its CUDA-event time
+    peaks, peaks_kind = measured_peaks()
+    clk_sum = clk.summary()
+    mhz = clk_sum.get("sm_mhz") or peaks.get("sm_max_mhz", 1965.0)
+    setup_s = stats["ms_setup"] / 1e3
+    achieved = SETUP_INST_PER_DIR * len(idx) / setup_s
+    peak = N_SM * SCHEDULERS * mhz * 1e6
+    roofline = {"kernel": "k_setup<32>", "bound": "issue", "achieved": achieved, "peak": peak,
+                "unit": "warp-inst/s", "frac": achieved / peak,
+                "traffic": SETUP_DRAM_PER_DIR * len(idx),
+                "basis": f"ncu: {SETUP_INST_PER_DIR:.0f} warp-inst and {SETUP_DRAM_PER_DIR:.0f} DRAM bytes per "
+                         f"direction; peak = {N_SM} SMs x {SCHEDULERS} x {mhz:.0f} MHz (sampled SM clock); "
+                         f"HBM for context: {peaks.get('hbm_gbs')} GB/s {peaks_kind}"}
     if rank == 0:
         line = {"metric": "lattice nodes/s", "value": value, "unit": "nodes/s", "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup,
@@ -326,7 +361,7 @@ def main():
                 "stage_ms": {"setup": stats["ms_setup"], "search": stats["ms_search"],
                              "output": stats["ms_output"]},
                 "fp32_nodes_per_step": stats["nodes"], "wall_ms_per_step": wall_s / args.steps * 1e3,
-                "clocks": clk.summary(), "e2e": e2e, "cpu_baseline": cpu,
+                "clocks": clk_sum, "e2e": e2e, "cpu_baseline": cpu, "roofline": roofline,
                 "gpu_launches": int(stats.get("launches", 0)) * args.steps}
         print(json.dumps(line))
     if pg is not None:

@@ -535,6 +535,9 @@ PFG_NOINLINE __device__ int warp_unimodular(const int64_t *vin, int n, int64_t *
 #ifndef PFG_DELTA_O
 #define PFG_DELTA_O 0.99        // LLL parameter of the Euclidean reduction of O
 #endif
+#ifndef PFG_DELTA_K
+#define PFG_DELTA_K 0.99        // LLL parameter of the cut-aware basis (the search basis)
+#endif
 
 // ---------------------------------------------------------------------------
 // The setup of one direction; S is the warp's LLL working set (N >= h11).
@@ -678,7 +681,7 @@ template <int N> __device__ int setup_one(const SetupArgs &A, int pid, int lane,
         if (warp_any(bad)) return ST_OVERFLOW;
         {
             Lll<N> LK{S, d, d};
-            if ((st = warp_lll(LK, d - 1, true, 0.99, lane))) return st;
+            if ((st = warp_lll(LK, d - 1, true, PFG_DELTA_K, lane))) return st;
         }
         // new columns a of Binter: sum_b B[a][b] Binter[:, b]  (likewise ZB)
         for (int e = lane; e < d * h; e += 32) {
