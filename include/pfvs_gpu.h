@@ -72,7 +72,8 @@ void pfg_output_free(pfg_output *out);
 /* Search form and pruning precision for pfg_coni_batch_ex. */
 enum {
     PFG_FORM_BATCHED = 0,      /* persistent work-stealing kernel over all directions */
-    PFG_FORM_PLAIN = 1         /* one launch per direction, one warp, no work sharing */
+    PFG_FORM_PLAIN = 1         /* one warp per direction (one block each, one launch), FP64
+                                  pruning, no work sharing: the plain form */
 };
 enum {
     PFG_PREC_AUTO = 0,         /* FP32 pruning where qmax < 2^22, FP64 retry on -11 */

@@ -427,19 +427,12 @@ extern "C" int pfg_coni_batch_ex(const pfg_input *in, const pfg_options *opt_in,
                 CK(cudaFuncSetAttribute(k_search<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, wpb32 * st32));
                 CK(cudaFuncSetAttribute(k_search<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, wpb64 * st64));
                 if (opt.form == PFG_FORM_PLAIN) {
-                    CK(cudaFuncSetAttribute(k_search_plain<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, st32));
+                    // one launch, one warp per direction, FP64 pruning, no work sharing
                     CK(cudaFuncSetAttribute(k_search_plain<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, st64));
-                    A.donate = 0; A.n_warps = 1;
-                    A.ctl = dctl;
-                    A.stage_bytes = st32;
-                    for (int k = 0; k < nb; ++k) {
-                        const bool f32 = geos[in->pgeo[off + k]].use_f32;
-                        if (f32) { k_search_plain<float><<<1, 32, st32>>>(A, k); ++launches; }
-                    }
-                    k_flip<<<(nb + 255) / 256, 256>>>(ddirs, dgeo, nb, 1, ddirpass, dretry); ++launches;
-                    A.pass = 2;
-                    A.stage_bytes = st64;
-                    for (int k = 0; k < nb; ++k) { k_search_plain<double><<<1, 32, st64>>>(A, k); ++launches; }
+                    k_flip<<<(nb + 255) / 256, 256>>>(ddirs, dgeo, nb, 0, ddirpass, dretry); ++launches;
+                    A.donate = 0; A.n_warps = 1; A.ctl = dctl + 1; A.pass = 2; A.stage_bytes = st64;
+                    A.todo = dtodoall; A.n_todo = nb;
+                    k_search_plain<double><<<nb, 32, st64>>>(A, -1); ++launches;
                     CK(cudaGetLastError());
                 } else {
                     auto grid_for = [&](const void *fn, int wpb, unsigned st, int &grid) -> cudaError_t {

@@ -252,14 +252,13 @@ template <class R> __device__ __forceinline__ void level_sums(const Lanes<R> &S,
     pre = hrow ? warp_sum128(pr) : (i128)0;
 }
 
-// Enter level i: candidate range [lo, hi] (lo > hi: none).  Returns
-// ST_RANGE if a bound leaves int32.
-template <class R> __device__ int enter_level(Lanes<R> &S, const Prob<R> &P, int i, R rem, R err, u128 gab,
-                                              int lane, int64_t &lo_o, int64_t &hi_o)
+// The candidate range [lo, hi] (lo > hi: none) of level i from its entry
+// values: remaining norm rem, its error bound err, the gcd bound gab of the
+// rows above, the centre offset off and the absolute sum aoff
+// (fpk_search_impl.h:241-348).  Returns ST_RANGE if a bound leaves int32.
+template <class R> __device__ __forceinline__ int level_range(const Prob<R> &P, int i, R rem, R err, u128 gab,
+                                                              R off, R aoff, int64_t &lo_o, int64_t &hi_o)
 {
-    R off, aoff;
-    i128 pre;
-    level_sums(S, P, i, lane, off, aoff, pre);
     const R slack = P.slack, Kerr = P.Kerr;
     R Rr = sqrt(fmax(rem + slack + err, (R)0));
     Rr += Kerr * (Rr + (R)2 * aoff) + Num<R>::tiny();
@@ -294,6 +293,21 @@ template <class R> __device__ int enter_level(Lanes<R> &S, const Prob<R> &P, int
             }
         }
     }
+    lo_o = lo; hi_o = hi;
+    return 0;
+}
+
+// Enter level i (warp search): the level's sums and candidate range into
+// the lanes' registers.  Returns ST_RANGE if a bound leaves int32.
+template <class R> __device__ int enter_level(Lanes<R> &S, const Prob<R> &P, int i, R rem, R err, u128 gab,
+                                              int lane, int64_t &lo_o, int64_t &hi_o)
+{
+    R off, aoff;
+    i128 pre;
+    level_sums(S, P, i, lane, off, aoff, pre);
+    int64_t lo, hi;
+    const int st = level_range(P, i, rem, err, gab, off, aoff, lo, hi);
+    if (st) return st;
     LSET(S, cur, i, lo); LSET(S, hi, i, hi);
     LSET(S, rem, i, rem); LSET(S, err, i, err);
     LSET(S, off, i, off); LSET(S, aoff, i, aoff);
@@ -630,10 +644,15 @@ __global__ void __launch_bounds__(256, 2) k_search(SearchArgs A)
     }
 }
 
-// The plain form: one direction per launch, one warp, no work sharing.
+// The plain form: one warp (block) per direction, no work sharing; pid < 0
+// takes the block's direction todo[blockIdx.x].
 template <class R>
 __global__ void __launch_bounds__(32) k_search_plain(SearchArgs A, int pid)
 {
+    if (pid < 0) {
+        if ((int)blockIdx.x >= A.n_todo) return;
+        pid = A.todo[blockIdx.x];
+    }
 #ifndef PFG_EMU
     extern __shared__ __align__(16) unsigned char pfg_stage_smem[];
 #endif

@@ -533,7 +533,10 @@ PFG_NOINLINE __device__ int warp_unimodular(const int64_t *vin, int n, int64_t *
 #define PFG_DELTA_H 0.99        // LLL parameter of the GCD-row reductions
 #endif
 #ifndef PFG_DELTA_O
-#define PFG_DELTA_O 0.99        // LLL parameter of the Euclidean reduction of O
+#define PFG_DELTA_O 0.5         // LLL parameter of the Euclidean reduction of O (it only has to
+                                // keep the entries small: the search basis is reduced again w.r.t.
+                                // mat with PFG_DELTA_K; 0.5 takes 14 % less setup time than 0.99 for
+                                // the same tree sizes)
 #endif
 #ifndef PFG_DELTA_K
 #define PFG_DELTA_K 0.99        // LLL parameter of the cut-aware basis (the search basis)

@@ -203,7 +203,7 @@ def coni_batch_multi_ex(geoms, ps, pgeo, device=0, batch=0, verbose=False,
                         warps_per_block=0, want_dir_nodes=False, gcd_min_tree=0.0):
     """
     `coni_batch_multi` with the search form (FORM_BATCHED: one persistent
-    work-stealing launch; FORM_PLAIN: one launch per direction), the pruning
+    work-stealing launch; FORM_PLAIN: one warp per direction in one launch, FP64 pruning, no work sharing), the pruning
     precision (PREC_AUTO: FP32 where qmax < 2^22 with an FP64 retry on -11;
     PREC_FP64) and the call's statistics.  Returns
     (M, Kn, q, pidx, pstat, seconds_gpu, stats dict[, dir_nodes]).
