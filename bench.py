@@ -45,8 +45,8 @@ sys.path.insert(0, ROOT)
 # SM clock.  Per-unit figures from one ncu capture of the kernel on the
 # first 16,384 directions of this batch (profiles/k_setup_mixed.md):
 # executed warp instructions and DRAM bytes per direction.
-SETUP_INST_PER_DIR = 23_323_134_329 / 16384
-SETUP_DRAM_PER_DIR = (64_152_064 + 526_142_464) / 16384
+SETUP_INST_PER_DIR = 17_400_906_604 / 16384
+SETUP_DRAM_PER_DIR = (95_471_616 + 593_945_856) / 16384
 N_SM, SCHEDULERS = 148, 4
 
 
