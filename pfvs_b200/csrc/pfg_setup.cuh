@@ -24,7 +24,7 @@
 //
 // The lattice reductions work on an LllMem<N> (rows of length <= N, the
 // exact Gram in int128 as a packed triangle, packed Gram-Schmidt data): for
-// h11 <= 32 it lives in shared memory (about 23 KB per warp), above that in
+// h11 <= 32 it lives in shared memory (20.8 KB per warp), above that in
 // the warp's global scratch.
 #pragma once
 #include "pfg_types.cuh"
@@ -35,7 +35,9 @@ namespace pfg {
 // LLL working set of one warp.
 // ---------------------------------------------------------------------------
 template <int N> struct LllMem {
-    static constexpr int R = N + 1;             // N basis rows + one 'last' row
+    static constexpr int R = N - 1;             // rows: at most d = h11 - 1 <= N - 1 are ever used
+                                                // (d basis rows in step 4; d - 1 plus the 'last'
+                                                // row in step 8; fewer in step 9)
     int64_t B[R * N];                           // rows, stride N
     i128 G[R * (R + 1) / 2];                    // exact Gram, lower triangle packed (gix)
     i128 T[R];                                  // a copied column of G / a temporary vector
