@@ -201,7 +201,7 @@ template <int N> PFG_NOINLINE __device__ int lll_reduce(Lll<N> &L, int k, int la
         double r0 = lane < k ? S->mu[mix(k, lane)] : 0.0;
         double r1 = 0.0;
         if (N > 32) r1 = lane + 32 < k ? S->mu[mix(k, lane + 32)] : 0.0;
-        bool any = false;
+        uint64_t qmask = 0;                             // rows j with q_j != 0 (uniform)
         for (int j = k - 1; j >= 0; --j) {
             const double x = __shfl_sync(FULL, (N > 32 && j >= 32) ? r1 : r0, j & 31);
             const double qd = rint(x);
@@ -209,11 +209,11 @@ template <int N> PFG_NOINLINE __device__ int lll_reduce(Lll<N> &L, int k, int la
             if (!(fabs(qd) <= 9.0e18)) return ST_OVERFLOW;
             if (lane == 0) S->q[j] = (int64_t)qd;
             if (qd == 0.0) continue;
-            any = true;
+            qmask |= 1ull << j;
             if (lane < j) r0 = fma(-qd, S->mu[mix(j, lane)], r0);
             if (N > 32 && lane + 32 < j) r1 = fma(-qd, S->mu[mix(j, lane + 32)], r1);
         }
-        if (!any) return 0;
+        if (!qmask) return 0;
         PFG_COUNT(2, 1);
         __syncwarp();                                   // q[] visible to all lanes
         bool bad = false;
@@ -221,16 +221,16 @@ template <int N> PFG_NOINLINE __device__ int lll_reduce(Lll<N> &L, int k, int la
         i128 b0 = 0, b1 = 0;
         if (lane < L.n) {
             b0 = S->B[k * N + lane];
-            for (int j = 0; j < k; ++j) {
-                const int64_t qj = S->q[j];
-                if (qj) bad |= submul_ovf(b0, qj, (i128)S->B[j * N + lane]);
+            for (uint64_t m = qmask; m; m &= m - 1) {
+                const int j = __ffsll((long long)m) - 1;
+                bad |= submul_ovf(b0, S->q[j], (i128)S->B[j * N + lane]);
             }
         }
         if (N > 32 && lane + 32 < L.n) {
             b1 = S->B[k * N + lane + 32];
-            for (int j = 0; j < k; ++j) {
-                const int64_t qj = S->q[j];
-                if (qj) bad |= submul_ovf(b1, qj, (i128)S->B[j * N + lane + 32]);
+            for (uint64_t m = qmask; m; m &= m - 1) {
+                const int j = __ffsll((long long)m) - 1;
+                bad |= submul_ovf(b1, S->q[j], (i128)S->B[j * N + lane + 32]);
             }
         }
         bad |= !fits64(b0) || !fits64(b1);
@@ -239,16 +239,16 @@ template <int N> PFG_NOINLINE __device__ int lll_reduce(Lll<N> &L, int k, int la
         i128 g0 = 0, g1 = 0;
         if (l0 < L.M && l0 != k) {
             g0 = S->G[gix(k, l0)];
-            for (int j = 0; j < k; ++j) {
-                const int64_t qj = S->q[j];
-                if (qj) bad |= submul_ovf(g0, qj, S->G[gix(j, l0)]);
+            for (uint64_t m = qmask; m; m &= m - 1) {
+                const int j = __ffsll((long long)m) - 1;
+                bad |= submul_ovf(g0, S->q[j], S->G[gix(j, l0)]);
             }
         }
         if (N > 32 && l1 < L.M && l1 != k) {
             g1 = S->G[gix(k, l1)];
-            for (int j = 0; j < k; ++j) {
-                const int64_t qj = S->q[j];
-                if (qj) bad |= submul_ovf(g1, qj, S->G[gix(j, l1)]);
+            for (uint64_t m = qmask; m; m &= m - 1) {
+                const int j = __ffsll((long long)m) - 1;
+                bad |= submul_ovf(g1, S->q[j], S->G[gix(j, l1)]);
             }
         }
         // G'(k, k) = G(k, k) - sum_{l<k} q_l (G(k, l) + G'(k, l))
