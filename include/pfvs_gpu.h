@@ -109,6 +109,32 @@ typedef struct {
 int pfg_coni_batch_ex(const pfg_input *in, const pfg_options *opt, pfg_output *out,
                       pfg_stats *stats, int64_t *dir_nodes);
 
+/* PFVs of a pfg_coni_pfvs call (arrays owned by the library). */
+typedef struct {
+    int64_t n;                 /* PFVs */
+    int64_t *K;                /* (n, pfg_max_h11()) row-major, first h11 entries valid */
+    int64_t *M;                /* (n, pfg_max_h11()) */
+    int64_t *pidx;             /* (n,) p-vector index */
+    int64_t n_points;          /* lattice points the post-processing started from */
+    int8_t *pstat;             /* (n_p,) 0 done, < 0 status as pfg_output's */
+    double seconds_gpu;
+    char err[256];
+} pfg_pfv_output;
+
+/* The batched pipeline followed by coniZpM's post-processing on the device:
+ * lattice points -> coni PFVs (K, M) exactly as the reference's
+ * _pfvs_from_points (pfvs/coni.py:275-412) computes them on the host from
+ * pfg_coni_batch's points: the strict GCD cut, the expansion over
+ * g = 1 .. (Q gcd(Kn[1:]) - 1) // q and K0, the tadpole check (a violation
+ * fails the call, as the reference raises), det((kappa.M)[1:, 1:]) != 0
+ * decided exactly, and the reference's order (p-vector, g, point, K0).
+ * No counterpart in the reference's C ABI.  M0min (linmin) must be > 0.
+ * Returns 0, or 1 with out->err set.  opt and stats may be NULL. */
+int pfg_coni_pfvs(const pfg_input *in, const pfg_options *opt, pfg_pfv_output *out, pfg_stats *stats);
+
+/* Free a pfg_pfv_output's arrays (safe on a zeroed struct). */
+void pfg_pfv_output_free(pfg_pfv_output *out);
+
 /*
  * No counterpart in the reference.  The coni pipeline for ONE p-vector,
  * for callers that cannot allocate device memory while they run (code in a

@@ -5,6 +5,7 @@
 //   k_flip       FP32 successes -> done; -11 -> FP64 retry
 //   k_search<d>  FP64-pruned search of the rest
 //   k_count .. k_rows      canonical output rows              (pfg_out.cuh)
+//   k_pfv_count .. k_pfv_rows   points -> PFVs (pfg_coni_pfvs)  (pfg_pfv.cuh)
 // with one host synchronisation at the end of a batch (point count, output
 // size).  No CPU fallback: a direction the device cannot finish exactly is
 // reported with a negative status.
@@ -25,6 +26,7 @@
 #include "pfg_setup.cuh"
 #include "pfg_search.cuh"
 #include "pfg_out.cuh"
+#include "pfg_pfv.cuh"
 
 using namespace pfg;
 
@@ -52,7 +54,8 @@ __global__ void k_fill_i32(int32_t *a, int32_t v, int n)
 enum {
     W_GEO, W_KAPPA, W_MB, W_PS, W_PGEO, W_SLABOFF, W_SLAB, W_DIRS, W_SCRATCH, W_TODO32, W_TODOALL, W_ORDER,
     W_CTL, W_ITEMS, W_READY, W_HDR, W_COORDS, W_DIRNODES, W_DIRPASS,
-    W_KEYS, W_COUNT, W_FILL, W_SEG, W_IDX, W_CSEG, W_SUM, W_PERM, W_PERM2, W_SIDX, W_OM, W_OK, W_OQ, W_OP, W_RETRY, W_N
+    W_KEYS, W_COUNT, W_FILL, W_SEG, W_IDX, W_CSEG, W_SUM, W_PERM, W_PERM2, W_SIDX, W_PCNT, W_PKG, W_PEPT, W_PEG, W_PEK0, W_PEORD, W_PNONS, W_PKEEP,
+    W_PERR, W_PSORT, W_PK, W_PM, W_PP, W_PRIMES, W_OM, W_OK, W_OQ, W_OP, W_RETRY, W_N
 };
 
 struct Workspace {
@@ -182,6 +185,48 @@ void chunk_free(Chunk &c)
     c = Chunk{nullptr, nullptr, nullptr, nullptr, 0};
 }
 
+// PFVs of a pfg_coni_pfvs call, per batch
+struct PfvChunk { int64_t *K, *M, *pidx; size_t n; };
+struct PfvSink {
+    std::vector<PfvChunk> chunks;
+    int64_t n_points = 0;
+    void release()
+    {
+        for (auto &c : chunks) for (int64_t *p : {c.K, c.M, c.pidx}) pinned_put(p);
+        chunks.clear();
+    }
+};
+
+// the first n primes below 2^31, descending (deterministic Miller-Rabin for
+// 32-bit numbers: bases 2, 3, 5, 7)
+bool is_prime32(uint32_t n)
+{
+    if (n < 2) return false;
+    for (uint32_t p : {2u, 3u, 5u, 7u}) if (n % p == 0) return n == p;
+    uint32_t d = n - 1;
+    int r = 0;
+    while (!(d & 1)) { d >>= 1; ++r; }
+    auto mulm = [n](uint64_t a, uint64_t b) { return (uint32_t)((a * b) % n); };
+    for (uint32_t a : {2u, 3u, 5u, 7u}) {
+        uint64_t x = 1, b = a, e = d;
+        while (e) { if (e & 1) x = mulm(x, b); b = mulm(b, b); e >>= 1; }
+        if (x == 1 || x == n - 1) continue;
+        bool comp = true;
+        for (int i = 1; i < r && comp; ++i) { x = mulm(x, x); if (x == n - 1) comp = false; }
+        if (comp) return false;
+    }
+    return true;
+}
+const std::vector<uint32_t> &primes31()
+{
+    static std::vector<uint32_t> P = [] {
+        std::vector<uint32_t> v;
+        for (uint32_t n = 2147483647u; v.size() < 64; n -= 2) if (is_prime32(n)) v.push_back(n);
+        return v;
+    }();
+    return P;
+}
+
 void set_err(pfg_output *out, const char *fmt, ...)
 {
     va_list ap;
@@ -246,8 +291,10 @@ extern "C" int pfg_coni_batch(const pfg_input *in, pfg_output *out)
     return pfg_coni_batch_ex(in, nullptr, out, nullptr, nullptr);
 }
 
-extern "C" int pfg_coni_batch_ex(const pfg_input *in, const pfg_options *opt_in, pfg_output *out,
-                                 pfg_stats *stats, int64_t *dir_nodes_out)
+// The pipeline over all batches: points into `out`, or, with `pfv`, the
+// points' PFVs into `pfv` (the points stay on the device).
+static int coni_run(const pfg_input *in, const pfg_options *opt_in, pfg_output *out, pfg_stats *stats,
+                    int64_t *dir_nodes_out, PfvSink *pfv)
 {
     memset(out, 0, sizeof *out);
     if (stats) memset(stats, 0, sizeof *stats);
@@ -537,8 +584,70 @@ extern "C" int pfg_coni_batch_ex(const pfg_input *in, const pfg_options *opt_in,
                 k_rows<<<nsm * 8, 256>>>(R); ++launches;
                 CK(cudaGetLastError());
             }
+            if (pfv && n_out) {
+                // ---- points -> PFVs (on the device) ----
+                pfv->n_points += (int64_t)n_out;
+                unsigned long long *pcnt, *pkeep; uint64_t *pkg; unsigned *pept, *peord, *psort;
+                int64_t *peg, *pek0; int *pnons, *perr; uint32_t *dprimes;
+                WS(pcnt, W_PCNT, (n_out + 1) * 8);
+                WS(pkg, W_PKG, n_out * 8);
+                WS(pnons, W_PNONS, n_out * 4);
+                WS(perr, W_PERR, 64);
+                WS(dprimes, W_PRIMES, primes31().size() * 4);
+                CK(cudaMemset(perr, 0, 64));
+                CK(cudaMemcpy(dprimes, primes31().data(), primes31().size() * 4, cudaMemcpyHostToDevice));
+                int hmax2 = 3;
+                for (int k = 0; k < nb; ++k) hmax2 = std::max(hmax2, geos[in->pgeo[off + k]].h);
+                PfvArgs PA{ddirs, dgeo, dkappa, oM, oK, oq, op, n_out, off, pcnt, pkg, nullptr, nullptr, nullptr,
+                           nullptr, pnons, nullptr, perr, dprimes, (int)primes31().size(), hmax2 - 1};
+                k_pfv_count<<<nsm * 4, 256>>>(PA); ++launches;
+                k_scan64<<<1, 1024>>>(pcnt, n_out); ++launches;
+                unsigned long long n_e = 0;
+                CK(cudaMemcpy(&n_e, pcnt + n_out, 8, cudaMemcpyDeviceToHost));
+                unsigned long long n_pfv = 0;
+                if (n_e) {
+                    unsigned np2 = 1;
+                    while (np2 < n_e) np2 <<= 1;
+                    WS(pept, W_PEPT, n_e * 4);
+                    WS(peg, W_PEG, n_e * 8);
+                    WS(pek0, W_PEK0, n_e * 8);
+                    WS(peord, W_PEORD, n_e * 4);
+                    WS(pkeep, W_PKEEP, (n_e + 1) * 8);
+                    WS(psort, W_PSORT, (size_t)np2 * 4);
+                    PA.e_pt = pept; PA.e_g = peg; PA.e_K0 = pek0; PA.e_ord = peord; PA.keep = pkeep;
+                    k_pfv_fill<<<nsm * 4, 256>>>(PA); ++launches;
+                    k_pfv_sort<<<1, 1024>>>(PA, n_e, np2, psort); ++launches;
+                    k_pfv_det<<<(int)std::min<unsigned long long>(n_out, (unsigned long long)nsm * 32), 32,
+                                (size_t)(hmax2 - 1) * (hmax2 - 1) * 4>>>(PA); ++launches;
+                    k_pfv_keep<<<nsm * 4, 256>>>(PA, n_e); ++launches;
+                    k_scan64<<<1, 1024>>>(pkeep, n_e); ++launches;
+                    CK(cudaGetLastError());
+                    CK(cudaMemcpy(&n_pfv, pkeep + n_e, 8, cudaMemcpyDeviceToHost));
+                }
+                int herr[3] = {0, 0, 0};
+                if (n_pfv) {
+                    int64_t *pK, *pM, *pP;
+                    WS(pK, W_PK, n_pfv * MH * 8);
+                    WS(pM, W_PM, n_pfv * MH * 8);
+                    WS(pP, W_PP, n_pfv * 8);
+                    k_pfv_rows<<<nsm * 8, 256>>>(PA, n_e, pK, pM, pP); ++launches;
+                    CK(cudaGetLastError());
+                    PfvChunk c{(int64_t *)pinned_get(n_pfv * MH * 8), (int64_t *)pinned_get(n_pfv * MH * 8),
+                               (int64_t *)pinned_get(n_pfv * 8), (size_t)n_pfv};
+                    pfv->chunks.push_back(c);
+                    if (!c.K || !c.M || !c.pidx) { set_err(out, "out of pinned host memory"); rc = 1; goto fail; }
+                    CK(cudaMemcpy(c.K, pK, n_pfv * MH * 8, cudaMemcpyDeviceToHost));
+                    CK(cudaMemcpy(c.M, pM, n_pfv * MH * 8, cudaMemcpyDeviceToHost));
+                    CK(cudaMemcpy(c.pidx, pP, n_pfv * 8, cudaMemcpyDeviceToHost));
+                }
+                CK(cudaMemcpy(herr, perr, sizeof herr, cudaMemcpyDeviceToHost));
+                if (herr[0]) { set_err(out, "Tadpole violation: -dot(K,M) > Q"); rc = 1; goto fail; }
+                if (herr[1] == 2) { set_err(out, "determinant test: more primes needed than provided"); rc = 1; goto fail; }
+                if (herr[1]) { set_err(out, "PFV entries beyond int64"); rc = 1; goto fail; }
+                if (herr[2]) { set_err(out, "a point expands over more than 2^22 values of g"); rc = 1; goto fail; }
+            }
             CK(cudaEventRecord(ev[4]));
-            if (n_out) {
+            if (n_out && !pfv) {
                 Chunk c{(int64_t *)pinned_get(n_out * MH * 8), (int64_t *)pinned_get(n_out * MH * 8),
                         (int64_t *)pinned_get(n_out * 8), (int64_t *)pinned_get(n_out * 8), (size_t)n_out};
                 chunks.push_back(c);
@@ -626,6 +735,73 @@ fail:
     if (rc) {
         cudaGetLastError();
         pfg_output_free(out);
+        if (pfv) pfv->release();
     }
     return rc;
+}
+
+extern "C" int pfg_coni_batch_ex(const pfg_input *in, const pfg_options *opt, pfg_output *out,
+                                 pfg_stats *stats, int64_t *dir_nodes)
+{
+    return coni_run(in, opt, out, stats, dir_nodes, nullptr);
+}
+
+extern "C" int pfg_coni_pfvs(const pfg_input *in, const pfg_options *opt, pfg_pfv_output *out, pfg_stats *stats)
+{
+    memset(out, 0, sizeof *out);
+    for (int gi = 0; gi < in->n_geo; ++gi)
+        if (in->linmin[gi] <= 0) {
+            snprintf(out->err, sizeof out->err, "coniZpM requires M0min > 0 (geometry %d)", gi);
+            return 1;
+        }
+    pfg_output pts;
+    PfvSink sink;
+    const int rc = coni_run(in, opt, &pts, stats, nullptr, &sink);
+    out->pstat = pts.pstat;
+    pts.pstat = nullptr;
+    out->seconds_gpu = pts.seconds_gpu;
+    out->n_points = sink.n_points;
+    if (rc) {
+        memcpy(out->err, pts.err, sizeof out->err);
+        sink.release();
+        pfg_output_free(&pts);
+        return rc;
+    }
+    pfg_output_free(&pts);
+    size_t n = 0;
+    for (auto &c : sink.chunks) n += c.n;
+    out->n = (int64_t)n;
+    if (sink.chunks.size() == 1) {
+        out->K = sink.chunks[0].K; out->M = sink.chunks[0].M; out->pidx = sink.chunks[0].pidx;
+        sink.chunks.clear();
+        return 0;
+    }
+    out->K = (int64_t *)pinned_get(n * MH * 8);
+    out->M = (int64_t *)pinned_get(n * MH * 8);
+    out->pidx = (int64_t *)pinned_get(n * 8);
+    if (!out->K || !out->M || !out->pidx) {
+        snprintf(out->err, sizeof out->err, "out of pinned host memory");
+        sink.release();
+        pfg_pfv_output_free(out);
+        return 1;
+    }
+    size_t base = 0;
+    for (auto &c : sink.chunks) {
+        memcpy(out->K + base * MH, c.K, c.n * MH * 8);
+        memcpy(out->M + base * MH, c.M, c.n * MH * 8);
+        memcpy(out->pidx + base, c.pidx, c.n * 8);
+        base += c.n;
+    }
+    sink.release();
+    return 0;
+}
+
+extern "C" void pfg_pfv_output_free(pfg_pfv_output *out)
+{
+    for (int64_t *p : {out->K, out->M, out->pidx})
+        if (!pinned_put(p)) free(p);
+    free(out->pstat);
+    out->K = out->M = out->pidx = nullptr;
+    out->pstat = nullptr;
+    out->n = 0;
 }

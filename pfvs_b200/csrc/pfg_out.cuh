@@ -18,9 +18,9 @@
 //   k_order    the sorted positions -> point indices
 //   k_rows     the MH-wide M and Kn rows, q and pidx in output order
 //
-// The rows are exact in int64: the setup guarantees |Binter|, |Z Binter| <
-// 2^25 and the search |c| < 2^31, so each product is below 2^56 and a sum of
-// at most 63 of them below 2^62.
+// The rows are exact in int64: the setup guarantees that every column of
+// Binter^T and (Z Binter)^T has an absolute sum below 2^31 (so each entry fits
+// int32) and the search |c| < 2^31, so every sum is below 2^62.
 #pragma once
 #include "pfg_types.cuh"
 

@@ -121,7 +121,7 @@ template <> struct Num<double> {
 
 // The search data of one direction, staged by the warp that searches it:
 // U packed by rows (upper triangle, row i holds U[i][i..d-1]), 1/U_ii, and
-// mat and ZB^T as int32 (the setup bounds their entries by 2^25); the
+// mat and ZB^T as int32 (the setup bounds their row / column absolute sums by 2^31); the
 // GCD-cut rows H stay in global memory (only large trees have them).
 PFG_HD int upk(int i, int j, int d) { return i * d - ((i * (i - 1)) >> 1) + (j - i); }
 template <class R> PFG_HD unsigned stage_bytes(int d, int h)

@@ -894,10 +894,27 @@ template <int N> __device__ int setup_one(const SetupArgs &A, int pid, int lane,
     }
 h_done:
     clk.mark(11);
-    // 11. the search keeps exact incremental sums mat c, ZB c, Binter c in int64
-    // (|entry| < 2^25, |c| < 2^31, <= 64 terms)
-    for (int e = lane; e < d * d; e += 32) bad |= uabs64(MAT[e]) >= (1ull << 25);
-    for (int e = lane; e < d * h; e += 32) bad |= uabs64(BT[e]) >= (1ull << 25) || uabs64(ZT[e]) >= (1ull << 25);
+    // 11. the search keeps exact sums mat c, ZB c, Binter c in int64 and stages
+    // mat and ZB^T as int32: every row of mat and every column of Binter^T and
+    // (Z Binter)^T has an absolute sum below 2^31, so with |c| < 2^31 every such
+    // sum (and every partial one) stays below 2^62
+    for (int r = lane; r < d; r += 32) {
+        uint64_t s = 0;
+        for (int j = 0; j < d; ++j) {
+            const uint64_t a = uabs64(MAT[r * d + j]);
+            if (a >= (1ull << 31)) bad = true; else s += a;
+        }
+        bad |= s >= (1ull << 31);
+    }
+    for (int r = lane; r < h; r += 32) {
+        uint64_t sb = 0, sz = 0;
+        for (int a = 0; a < d; ++a) {
+            const uint64_t x = uabs64(BT[a * h + r]), y = uabs64(ZT[a * h + r]);
+            if (x >= (1ull << 31) || y >= (1ull << 31)) bad = true;
+            else { sb += x; sz += y; }
+        }
+        bad |= sb >= (1ull << 31) || sz >= (1ull << 31);
+    }
     if (warp_any(bad)) return ST_OVERFLOW;
     if (lane == 0) {
         D.m0_level = m0_level;

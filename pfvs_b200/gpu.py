@@ -50,6 +50,12 @@ class _Options(ctypes.Structure):
                 ("gcd_min_tree", ctypes.c_double)]
 
 
+class _PfvOutput(ctypes.Structure):
+    _fields_ = [("n", ctypes.c_int64), ("K", _i64p), ("M", _i64p), ("pidx", _i64p),
+                ("n_points", ctypes.c_int64), ("pstat", ctypes.POINTER(ctypes.c_int8)),
+                ("seconds_gpu", ctypes.c_double), ("err", ctypes.c_char * 256)]
+
+
 class _Stats(ctypes.Structure):
     _fields_ = [("nodes", ctypes.c_int64), ("candidates", ctypes.c_int64),
                 ("leaves", ctypes.c_int64), ("points", ctypes.c_int64),
@@ -98,6 +104,10 @@ def _load():
                                       ctypes.POINTER(_Output), ctypes.POINTER(_Stats), _i64p]
     lib.pfg_coni_batch_ex.restype = ctypes.c_int
     lib.pfg_output_free.argtypes = [ctypes.POINTER(_Output)]
+    lib.pfg_coni_pfvs.argtypes = [ctypes.POINTER(_Input), ctypes.POINTER(_Options),
+                                  ctypes.POINTER(_PfvOutput), ctypes.POINTER(_Stats)]
+    lib.pfg_coni_pfvs.restype = ctypes.c_int
+    lib.pfg_pfv_output_free.argtypes = [ctypes.POINTER(_PfvOutput)]
     lib.pfg_release.argtypes = [ctypes.c_int]
     _lib = lib
     return lib
@@ -236,6 +246,56 @@ def coni_batch_multi_ex(geoms, ps, pgeo, device=0, batch=0, verbose=False,
     del owner
     res = (M, Kn, q, pidx, pstat.astype(np.int8), secs, st.as_dict())
     return res + (dn[:n_p],) if want_dir_nodes else res
+
+
+class _PfvOwner:
+    """Owns one pfg_pfv_output; frees it (pfg_pfv_output_free) when collected."""
+
+    def __init__(self, lib, out):
+        self.lib, self.out = lib, out
+
+    def __del__(self):
+        try:
+            self.lib.pfg_pfv_output_free(ctypes.byref(self.out))
+        except Exception:
+            pass
+
+
+def coni_pfvs_multi(geoms, ps, pgeo, device=0, batch=0, verbose=False, form=FORM_BATCHED,
+                    precision=PREC_AUTO, gcd_min_tree=0.0):
+    """
+    The batched pipeline and coniZpM's post-processing (pfvs/coni.py:275-412,
+    `_pfvs_from_points`), both on the device: the coni PFVs of every
+    p-vector.  Arguments as `coni_batch_multi` (M0min > 0).  Returns
+    (Ks, Ms, pidx, pstat, seconds_gpu, stats dict): Ks, Ms of shape
+    (n, max_h11()) (first h11 entries valid), grouped by p-vector (ascending)
+    in the reference's order within one.
+    """
+    lib = _require()
+    MH = lib.pfg_max_h11()
+    h, Q, qmax, linmin, kap, Mb, P, pgeo, n_p = _pack(geoms, ps, pgeo, MH)
+    inp = _Input(len(geoms), h.ctypes.data_as(_i32p), Q.ctypes.data_as(_i64p),
+                 qmax.ctypes.data_as(_i64p), linmin.ctypes.data_as(_i64p),
+                 kap.ctypes.data_as(_i64p), Mb.ctypes.data_as(_i64p),
+                 n_p, P.ctypes.data_as(_i64p), pgeo.ctypes.data_as(_i32p),
+                 int(device), int(batch), int(bool(verbose)))
+    opt = _Options(int(form), int(precision), 0, 0, float(gcd_min_tree))
+    st = _Stats()
+    out = _PfvOutput()
+    rc = lib.pfg_coni_pfvs(ctypes.byref(inp), ctypes.byref(opt), ctypes.byref(out), ctypes.byref(st))
+    if rc != 0:
+        raise RuntimeError(f"GPU pipeline failed: {out.err.decode(errors='replace')}")
+    owner = _PfvOwner(lib, out)
+    n = out.n
+    K, M = _view(owner, out.K, (n, MH)), _view(owner, out.M, (n, MH))
+    pidx = _view(owner, out.pidx, (n,))
+    pstat = np.ctypeslib.as_array(out.pstat, shape=(n_p,)).copy() if n_p \
+        else np.zeros(0, dtype=np.int8)
+    stats = st.as_dict()
+    stats["points"] = out.n_points
+    secs = out.seconds_gpu
+    del owner
+    return K, M, pidx, pstat.astype(np.int8), secs, stats
 
 
 def coni_batch_multi(geoms, ps, pgeo, device=0, batch=0, verbose=False):

@@ -112,7 +112,8 @@ def test_oracle_matches_reference_build(name, n, dils):
     assert_same(a, b, ok_mask=b[4] == 0)
 
 
-GOLDEN = sorted(f[:-4] for f in os.listdir(os.path.join(ROOT, "tests", "golden")) if f.endswith(".npz"))
+GOLDEN = sorted(f[:-4] for f in os.listdir(os.path.join(ROOT, "tests", "golden"))
+                if f.endswith(".npz") and f != "dataset_pfvs.npz")
 
 
 @pytest.mark.parametrize("key", GOLDEN)
@@ -184,3 +185,24 @@ def test_device_code_under_warp_emulator():
     got = emu.coni_batch_multi(geoms, ps, pgeo)
     assert np.all(got[4] == 0) and len(got[2]) == 51
     assert_same(got[:4], expected(geoms, ps, pgeo, "oracle"))
+
+
+def test_device_code_under_warp_emulator_on_dataset_geometries():
+    """The device sources (CPU warp emulator) on the reference's own coni
+    dataset geometries (tests/golden/dataset_pfvs.npz, h11 3..9): the first
+    4 p-vectors of each of the 30 geometries, points equal to the oracle's."""
+    from emu import emu
+    G = np.load(os.path.join(ROOT, "tests", "golden", "dataset_pfvs.npz"))
+    geoms, ps, pgeo = [], [], []
+    for k in range(int(G["n_geometries"][0])):
+        h, Q, m0 = (int(x) for x in G[f"g{k}_scal"])
+        geoms.append(dict(kappa=G[f"g{k}_kappa"], Mbasis=G[f"g{k}_Mbasis"], Q=Q,
+                          dilation=float(G[f"g{k}_D"][0]), M0min=m0))
+        for p in G[f"g{k}_ps"][:4]:
+            ps.append(np.asarray(p, dtype=np.int64))
+            pgeo.append(k)
+    pgeo = np.array(pgeo, dtype=np.int32)
+    got = emu.coni_batch_multi(geoms, ps, pgeo)
+    assert np.all(got[4] == 0) and len(got[2]) > 20
+    assert_same(got[:4], expected(geoms, ps, pgeo, "oracle"))
+
