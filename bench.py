@@ -329,6 +329,14 @@ def main():
                    "sample": f"{len(pick)} random directions (seed 1) of the batch, "
                              f"{dt:.1f} s on {threads} threads; the reference's own tree nodes",
                    "directions_per_s": rd / dt}
+    # PFVs: the same batch through the device post-processing (pfg_coni_pfvs), once, untimed
+    pfv = None
+    if not args.no_e2e:
+        Kp, Mp, pp, sp, secs_p, st_p = gpu.coni_pfvs_multi(geoms, ps, pgeo, device=device)
+        pfv = {"pfvs_per_step": int(allsum(pg, len(pp))), "points_in": int(allsum(pg, st_p["points"])),
+               "device_ms": allmax(pg, secs_p) * 1e3,
+               "pfvs_per_s": allsum(pg, len(pp)) / max(allmax(pg, secs_p), 1e-12)}
+        del Kp, Mp, pp
     # roofline of the setup kernel: executed warp instructions per launch (ncu
     # per-direction figure x directions) over its CUDA-event time
     peaks, peaks_kind = measured_peaks()
@@ -361,7 +369,7 @@ def main():
                 "stage_ms": {"setup": stats["ms_setup"], "search": stats["ms_search"],
                              "output": stats["ms_output"]},
                 "fp32_nodes_per_step": stats["nodes"], "wall_ms_per_step": wall_s / args.steps * 1e3,
-                "clocks": clk_sum, "e2e": e2e, "cpu_baseline": cpu, "roofline": roofline,
+                "clocks": clk_sum, "e2e": e2e, "cpu_baseline": cpu, "roofline": roofline, "pfvs": pfv,
                 "gpu_launches": int(stats.get("launches", 0)) * args.steps}
         print(json.dumps(line))
     if pg is not None:
