@@ -67,7 +67,7 @@ def parse():
     ap.add_argument("--workload", default="mixed")
     ap.add_argument("--n", type=int, default=0, help="directions per GPU (0: the workload's size)")
     ap.add_argument("--form", default="batched", choices=["batched", "plain"])
-    ap.add_argument("--precision", default="auto", choices=["auto", "fp64"])
+    ap.add_argument("--precision", default="auto", choices=["auto", "fp64", "fp32"])
     ap.add_argument("--cpu-sample", type=int, default=0, help="directions in the CPU sample (0: auto)")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
@@ -267,7 +267,7 @@ def main():
     w, idx = workload_slice(args.workload, n_total, rank, world)
     geoms, ps, pgeo = layout(w, idx)
     form = gpu.FORM_PLAIN if args.form == "plain" else gpu.FORM_BATCHED
-    prec = gpu.PREC_FP64 if args.precision == "fp64" else gpu.PREC_AUTO
+    prec = {"auto": gpu.PREC_AUTO, "fp64": gpu.PREC_FP64, "fp32": gpu.PREC_FP32}[args.precision]
 
     # work unit: nodes of the FP64-pruned tree with every GCD-cut row built (the
     # reference's pruning), counted once, untimed; the timed steps build the

@@ -76,9 +76,11 @@ enum {
                                   pruning, no work sharing: the plain form */
 };
 enum {
-    PFG_PREC_AUTO = 0,         /* FP32 pruning where qmax < 2^22, FP64 retry on -11 */
+    PFG_PREC_AUTO = 0,         /* the library's choice: FP64 on this build (the search is
+                                  latency-bound, so FP32 pruning gains nothing and its
+                                  FP64 retries cost; measured on B200) */
     PFG_PREC_FP64 = 1,         /* FP64 pruning everywhere */
-    PFG_PREC_FP32 = 2          /* as AUTO */
+    PFG_PREC_FP32 = 2          /* FP32 pruning where qmax < 2^22, FP64 retry on -11 */
 };
 
 typedef struct {

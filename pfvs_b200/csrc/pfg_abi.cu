@@ -316,7 +316,7 @@ static int coni_run(const pfg_input *in, const pfg_options *opt_in, pfg_output *
                 set_err(out, "geometry %d: unsupported h11 = %d (3..%d), Q or qmax", gi, g.h, MH);
                 return 1;
             }
-            g.use_f32 = g.qmax < (1LL << 22) && opt.precision != PFG_PREC_FP64;
+            g.use_f32 = g.qmax < (1LL << 22) && opt.precision == PFG_PREC_FP32;
             g.koff = koff; g.moff = moff;
             g.slab_len = slab_layout(g.h, g.d).len;
             koff += (int64_t)g.h * g.h * g.h;
@@ -618,7 +618,7 @@ static int coni_run(const pfg_input *in, const pfg_options *opt_in, pfg_output *
                     k_pfv_fill<<<nsm * 4, 256>>>(PA); ++launches;
                     k_pfv_sort<<<1, 1024>>>(PA, n_e, np2, psort); ++launches;
                     k_pfv_det<<<(int)std::min<unsigned long long>(n_out, (unsigned long long)nsm * 32), 32,
-                                (size_t)(hmax2 - 1) * (hmax2 - 1) * 4>>>(PA); ++launches;
+                                (size_t)(hmax2 - 1) * (hmax2 - 1) * 12>>>(PA); ++launches;
                     k_pfv_keep<<<nsm * 4, 256>>>(PA, n_e); ++launches;
                     k_scan64<<<1, 1024>>>(pkeep, n_e); ++launches;
                     CK(cudaGetLastError());

@@ -48,7 +48,7 @@ struct PfvArgs {
     int mmax;                        // largest h11 - 1 of the batch (det matrix size)
 };
 
-constexpr long long PFV_MAX_G = 1ll << 22;     // longest g expansion of one point
+constexpr long long PFV_MAX_G = 1ll << 22;     // most candidate g of one point
 
 __device__ __forceinline__ bool pfv_prep(const PfvArgs &P, unsigned long long t, int &h, int64_t &Q, uint64_t &Kg,
                                          i128 &gcap, i128 &raw, int64_t &nat_K0, int64_t &M0)
@@ -71,15 +71,57 @@ __device__ __forceinline__ bool pfv_prep(const PfvArgs &P, unsigned long long t,
     return M0 > 0;
 }
 
-// (lo, up) of K0 for expansion g; empty when lo > up
-__device__ __forceinline__ void pfv_range(i128 g, i128 raw, int64_t Q, int64_t M0, int64_t nat_K0, uint64_t Kg,
-                                          i128 &lo, i128 &up)
+// The K0 range of expansion g is non-empty only when M0 divides g raw - Q
+// (its ends are ceil and floor of (g raw - Q) / M0), i.e. g raw = Q (mod M0):
+// the first such g >= 1 and the step between them, or false if there is none.
+__device__ __forceinline__ bool pfv_g_progression(i128 raw, int64_t Q, int64_t M0, i128 &g0, i128 &step)
 {
-    const i128 x = g * raw - (i128)Q;
-    lo = -fdiv128(-x, (i128)M0);
-    up = fdiv128(x, (i128)M0);
-    const i128 cap = -fdiv128(-(i128)nat_K0 * g, (i128)Kg) - 1;
-    if (cap < up) up = cap;
+    const i128 m = M0;
+    i128 r = raw % m;
+    if (r < 0) r += m;
+    i128 qm = (i128)Q % m;
+    if (qm < 0) qm += m;
+    // d = gcd(r, m); solvable iff d | qm
+    i128 a = r, b = m;
+    while (b) { const i128 t = a % b; a = b; b = t; }
+    const i128 d = a;                               // (r = 0: d = m)
+    if (qm % d) return false;
+    const i128 m2 = m / d, r2 = r / d, q2 = qm / d;
+    // inverse of r2 modulo m2 (extended Euclid)
+    i128 x0 = 1, x1 = 0, a0 = r2 % m2, a1 = m2;
+    while (a1) {
+        const i128 qq = a0 / a1, t = a0 - qq * a1;
+        a0 = a1; a1 = t;
+        const i128 tx = x0 - qq * x1;
+        x0 = x1; x1 = tx;
+    }
+    i128 inv = m2 > 1 ? x0 % m2 : 0;
+    if (inv < 0) inv += m2;
+    i128 g = m2 > 1 ? (q2 % m2) * inv % m2 : 0;
+    if (g < 1) g += m2;
+    g0 = g;
+    step = m2;
+    return true;
+}
+
+// The entries of a point in closed form.  For g in the progression above,
+// K0 = (g raw - Q) / M0 exactly, and the cap K0 <= ceil(Kn0 g / Kg) - 1 is
+// K0 Kg < Kn0 g, i.e. g (raw Kg - M0 Kn0) < Q Kg: with c = raw Kg - M0 Kn0,
+// every g <= (Q Kg - 1) // c when c > 0, every g otherwise; and g <= gcap.
+// Returns the number of entries; g0, step as pfv_g_progression.
+__device__ __forceinline__ unsigned long long pfv_entries(i128 gcap, i128 raw, int64_t Q, int64_t M0, int64_t nat_K0,
+                                                          uint64_t Kg, i128 &g0, i128 &step)
+{
+    if (!pfv_g_progression(raw, Q, M0, g0, step)) return 0;
+    i128 G = gcap;
+    const i128 c = raw * (i128)Kg - (i128)M0 * nat_K0, QK = (i128)Q * (i128)Kg;
+    if (c > 0) {
+        const i128 gc = (QK - 1) / c;
+        if (gc < G) G = gc;
+    }
+    if (G < g0) return 0;
+    const i128 n = (G - g0) / step + 1;
+    return n > (i128)PFV_MAX_G ? ~0ull : (unsigned long long)n;
 }
 
 __global__ void k_pfv_count(PfvArgs P)
@@ -89,15 +131,11 @@ __global__ void k_pfv_count(PfvArgs P)
         int h;
         int64_t Q, nat_K0, M0;
         uint64_t Kg;
-        i128 gcap, raw;
+        i128 gcap, raw, g0, step;
         unsigned long long c = 0;
         if (pfv_prep(P, t, h, Q, Kg, gcap, raw, nat_K0, M0)) {
-            if (gcap > (i128)PFV_MAX_G) { atomicExch(&P.err[2], 1); gcap = 0; }
-            for (i128 g = 1; g <= gcap; ++g) {
-                i128 lo, up;
-                pfv_range(g, raw, Q, M0, nat_K0, Kg, lo, up);
-                if (lo <= up) c += (unsigned long long)(up - lo + 1);
-            }
+            c = pfv_entries(gcap, raw, Q, M0, nat_K0, Kg, g0, step);
+            if (c == ~0ull) { atomicExch(&P.err[2], 1); c = 0; }
         }
         P.Kg[t] = Kg;
         P.cnt[t] = c;
@@ -130,22 +168,22 @@ __global__ void k_pfv_fill(PfvArgs P)
     for (unsigned long long t = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; t < P.n;
          t += (unsigned long long)gridDim.x * blockDim.x) {
         unsigned long long pos = P.cnt[t];
-        if (P.cnt[t + 1] == pos) continue;
+        const unsigned long long n = P.cnt[t + 1] - pos;
+        if (!n) continue;
         int h;
         int64_t Q, nat_K0, M0;
         uint64_t Kg;
-        i128 gcap, raw;
+        i128 gcap, raw, g0, step;
         if (!pfv_prep(P, t, h, Q, Kg, gcap, raw, nat_K0, M0)) continue;
-        for (i128 g = 1; g <= gcap; ++g) {
-            i128 lo, up;
-            pfv_range(g, raw, Q, M0, nat_K0, Kg, lo, up);
-            for (i128 k0 = lo; k0 <= up; ++k0) {
-                if (!fits64(k0)) { atomicExch(&P.err[1], 1); continue; }
-                P.e_pt[pos] = (unsigned)t;
-                P.e_g[pos] = (int64_t)g;
-                P.e_K0[pos] = (int64_t)k0;
-                ++pos;
-            }
+        if (!pfv_g_progression(raw, Q, M0, g0, step)) continue;
+        for (unsigned long long j = 0; j < n; ++j) {
+            const i128 g = g0 + (i128)j * step;
+            const i128 k0 = (g * raw - (i128)Q) / (i128)M0;       // exact
+            if (!fits64(k0)) { atomicExch(&P.err[1], 1); continue; }
+            P.e_pt[pos] = (unsigned)t;
+            P.e_g[pos] = (int64_t)g;
+            P.e_K0[pos] = (int64_t)k0;
+            ++pos;
         }
     }
 }
@@ -185,30 +223,40 @@ __global__ void __launch_bounds__(1024) k_pfv_sort(PfvArgs P, unsigned long long
     for (unsigned t = threadIdx.x; t < n_e; t += blockDim.x) P.e_ord[t] = a[t];
 }
 
-__device__ __forceinline__ uint32_t mulmod(uint32_t a, uint32_t b, uint32_t p)
-{
-    return (uint32_t)(((uint64_t)a * b) % p);
-}
-__device__ __forceinline__ uint32_t powmod(uint32_t a, uint32_t e, uint32_t p)
-{
-    uint32_t r = 1;
-    while (e) {
-        if (e & 1) r = mulmod(r, a, p);
-        a = mulmod(a, a, p);
-        e >>= 1;
+// arithmetic modulo a prime p < 2^31 with Barrett reduction (x < 2^64)
+struct ModP {
+    uint32_t p;
+    uint64_t m;                                     // floor((2^64 - 1) / p)
+    __device__ explicit ModP(uint32_t p_) : p(p_), m(~0ull / p_) {}
+    __device__ __forceinline__ uint32_t red(uint64_t x) const
+    {
+        uint64_t r = x - __umul64hi(x, m) * (uint64_t)p;
+        while (r >= p) r -= p;
+        return (uint32_t)r;
     }
-    return r;
-}
-__device__ __forceinline__ uint32_t modp(int64_t x, uint32_t p)
-{
-    const int64_t r = x % (int64_t)p;
-    return (uint32_t)(r < 0 ? r + p : r);
-}
+    __device__ __forceinline__ uint32_t mul(uint32_t a, uint32_t b) const { return red((uint64_t)a * b); }
+    __device__ __forceinline__ uint32_t of(int64_t x) const
+    {
+        const uint32_t r = red(uabs64(x));
+        return x < 0 && r ? p - r : r;
+    }
+    __device__ uint32_t pow(uint32_t a, uint32_t e) const
+    {
+        uint32_t r = 1;
+        while (e) {
+            if (e & 1) r = mul(r, a);
+            a = mul(a, a);
+            e >>= 1;
+        }
+        return r;
+    }
+};
 
 // det(A) mod p for the m x m matrix in shared memory A (row stride m), lanes
 // own columns; A is destroyed
-__device__ uint32_t warp_det_mod(uint32_t *A, int m, uint32_t p, int lane)
+__device__ uint32_t warp_det_mod(uint32_t *A, int m, const ModP &F, int lane)
 {
+    const uint32_t p = F.p;
     uint32_t det = 1;
     for (int c = 0; c < m; ++c) {
         const bool nz0 = lane >= c && lane < m && A[lane * m + c] != 0;
@@ -227,14 +275,14 @@ __device__ uint32_t warp_det_mod(uint32_t *A, int m, uint32_t p, int lane)
             __syncwarp();
         }
         const uint32_t piv = A[c * m + c];
-        det = mulmod(det, piv, p);
-        const uint32_t inv = powmod(piv, p - 2, p);
+        det = F.mul(det, piv);
+        const uint32_t inv = F.pow(piv, p - 2);
         for (int i = c + 1; i < m; ++i) {
-            const uint32_t f = mulmod(A[i * m + c], inv, p);
+            const uint32_t f = F.mul(A[i * m + c], inv);
             if (f) {
-                const uint32_t nf = p - f;
+                const uint64_t nf = p - f;
                 for (int j = c + 1 + lane; j < m; j += 32)
-                    A[i * m + j] = (uint32_t)((A[i * m + j] + (uint64_t)nf * A[c * m + j]) % p);
+                    A[i * m + j] = F.red(A[i * m + j] + nf * A[c * m + j]);
             }
         }
         __syncwarp();
@@ -246,9 +294,11 @@ __device__ uint32_t warp_det_mod(uint32_t *A, int m, uint32_t p, int lane)
 __global__ void __launch_bounds__(32) k_pfv_det(PfvArgs P)
 {
 #ifdef PFG_EMU
+    static int64_t Nx[MD * MD];
     static uint32_t A[MD * MD];
 #else
-    extern __shared__ __align__(16) uint32_t A[];
+    extern __shared__ __align__(16) int64_t Nx[];                  // exact matrix (mmax^2)
+    uint32_t *A = (uint32_t *)(Nx + P.mmax * P.mmax);              // its residues (mmax^2)
 #endif
     const int lane = threadIdx.x & 31;
     for (unsigned long long t = blockIdx.x; t < P.n; t += gridDim.x) {
@@ -271,19 +321,34 @@ __global__ void __launch_bounds__(32) k_pfv_det(PfvArgs P)
         }
         for (int o = 16; o; o >>= 1) lb += __shfl_xor_sync(FULL, lb, o);
         lb = lb * (1.0 + 1e-9) + 2.0;                   // (det = 0 iff |det| < prod p / 2)
+        // the exact matrix once (int64 when it fits; otherwise residues are built per prime)
+        bool big = false;
+        for (int e = lane; e < m * m; e += 32) {
+            const int i = e / m, j = e % m;
+            const int64_t *kr = kap + ((int64_t)(i + 1) * h + (j + 1)) * h;
+            i128 s = 0, t;
+            for (int k = 0; k < h; ++k)
+                if (mul_ovf((i128)kr[k], (i128)Mt[k], &t) || add_ovf(s, t, &s)) big = true;
+            if (!fits64(s)) big = true;
+            Nx[e] = (int64_t)s;
+        }
+        big = __any_sync(FULL, big);
+        __syncwarp();
         int res = -1;
         double covered = 0.0;
         for (int pi = 0; pi < P.n_primes && res < 0; ++pi) {
-            const uint32_t p = P.primes[pi];
+            const ModP F(P.primes[pi]);
+            const uint32_t p = F.p;
             for (int e = lane; e < m * m; e += 32) {
+                if (!big) { A[e] = F.of(Nx[e]); continue; }
                 const int i = e / m, j = e % m;
-                uint32_t s = 0;
                 const int64_t *kr = kap + ((int64_t)(i + 1) * h + (j + 1)) * h;
-                for (int k = 0; k < h; ++k) s = (uint32_t)((s + (uint64_t)modp(kr[k], p) * modp(Mt[k], p)) % p);
+                uint32_t s = 0;
+                for (int k = 0; k < h; ++k) s = F.red((uint64_t)s + (uint64_t)F.mul(F.of(kr[k]), F.of(Mt[k])));
                 A[e] = s;
             }
             __syncwarp();
-            const uint32_t dp = warp_det_mod(A, m, p, lane);
+            const uint32_t dp = warp_det_mod(A, m, F, lane);
             if (dp != 0) res = 1;
             else {
                 covered += log2((double)p);

@@ -214,8 +214,9 @@ def coni_batch_multi_ex(geoms, ps, pgeo, device=0, batch=0, verbose=False,
     """
     `coni_batch_multi` with the search form (FORM_BATCHED: one persistent
     work-stealing launch; FORM_PLAIN: one warp per direction in one launch, FP64 pruning, no work sharing), the pruning
-    precision (PREC_AUTO: FP32 where qmax < 2^22 with an FP64 retry on -11;
-    PREC_FP64) and the call's statistics.  Returns
+    precision (PREC_AUTO: the library's choice, FP64 on B200; PREC_FP64;
+    PREC_FP32: FP32 where qmax < 2^22 with an FP64 retry on -11) and the
+    call's statistics.  Returns
     (M, Kn, q, pidx, pstat, seconds_gpu, stats dict[, dir_nodes]).
     """
     lib = _require()

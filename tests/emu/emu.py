@@ -40,8 +40,9 @@ def _load():
     return _lib
 
 
-def coni_batch_multi(geoms, ps, pgeo, precision=0, n_warps=2):
-    """As pfvs_b200.gpu.coni_batch_multi, on the emulated warps.  Returns
+def coni_batch_multi(geoms, ps, pgeo, precision=2, n_warps=2):
+    """As pfvs_b200.gpu.coni_batch_multi, on the emulated warps (default: FP32
+    pruning with the FP64 retry, so that both search instantiations run).  Returns
     (M, Kn, q, pidx, pstat, dir_nodes, setup_failure_stage)."""
     from pfvs_b200 import gpu
     lib = _load()

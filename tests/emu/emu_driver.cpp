@@ -39,7 +39,7 @@ extern "C" int emu_coni_batch(const pfg_input *in, int precision, int n_warps, p
         Geo &g = geos[gi];
         g.h = in->h[gi]; g.d = g.h - 1;
         g.Q = in->Q[gi]; g.qmax = in->qmax[gi]; g.linmin = in->linmin[gi];
-        g.use_f32 = g.qmax < (1LL << 22) && precision != PFG_PREC_FP64;
+        g.use_f32 = g.qmax < (1LL << 22) && precision == PFG_PREC_FP32;
         g.koff = koff; g.moff = moff;
         g.slab_len = slab_layout(g.h, g.d).len;
         koff += (int64_t)g.h * g.h * g.h;

@@ -67,7 +67,7 @@ def test_forms_and_precisions_agree(case):
     name, n, dils = case
     w = workloads.build(name, n_p=n, dilations=dils)
     geoms, ps, pgeo, hs = layout(w)
-    a = gpu.coni_batch_multi_ex(geoms, ps, pgeo, precision=gpu.PREC_AUTO)
+    a = gpu.coni_batch_multi_ex(geoms, ps, pgeo, precision=gpu.PREC_FP32)
     b = gpu.coni_batch_multi_ex(geoms, ps, pgeo, precision=gpu.PREC_FP64)
     c = gpu.coni_batch_multi_ex(geoms, ps, pgeo, form=gpu.FORM_PLAIN, precision=gpu.PREC_FP64)
     for x in (b, c):
