@@ -265,7 +265,11 @@ def main():
     device = local
     n_total = (args.n * world) if args.n else None
     w, idx = workload_slice(args.workload, n_total, rank, world)
-    geoms, ps, pgeo = layout(w, idx)
+    geoms, ps_list, pgeo = layout(w, idx)
+    # the p-vectors as one zero-padded 2-D array, the form the reference's coniZpM passes
+    ps = np.zeros((len(ps_list), max((len(p) for p in ps_list), default=1)), dtype=np.int64)
+    for i, p in enumerate(ps_list):
+        ps[i, :len(p)] = p
     form = gpu.FORM_PLAIN if args.form == "plain" else gpu.FORM_BATCHED
     prec = {"auto": gpu.PREC_AUTO, "fp64": gpu.PREC_FP64, "fp32": gpu.PREC_FP32}[args.precision]
 

@@ -571,7 +571,7 @@ static int coni_run(const pfg_input *in, const pfg_options *opt_in, pfg_output *
             if (n_out) {
                 const int smem_sort = SORT_CAP * KEYN * 8 + SORT_CAP * 4;
                 CK(cudaFuncSetAttribute(k_segsort, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_sort));
-                k_keys<<<nsm * 4, 256>>>(O, n_out); ++launches;
+                k_keys<<<nsm * 8, 256>>>(O, n_out); ++launches;
                 k_segsort<<<(int)std::min<unsigned long long>(n_chunks, (unsigned long long)nsm * 3), 256,
                             smem_sort>>>(O); ++launches;
                 unsigned *pin = dperm, *pout = dperm2;
@@ -579,8 +579,8 @@ static int coni_run(const pfg_input *in, const pfg_options *opt_in, pfg_output *
                     k_merge<<<nsm * 8, 256>>>(O, n_out, (unsigned)L, pin, pout); ++launches;
                     std::swap(pin, pout);
                 }
-                k_order<<<nsm * 4, 256>>>(O, n_out, pin, dsidx); ++launches;
-                RowArgs R{ddirs, dslab, dhdr, dcoords, dsidx, n_out, off, oM, oK, oq, op};
+                k_order<<<nsm * 4, 256>>>(O, n_out, pin, dsidx, pout); ++launches;
+                RowArgs R{ddirs, dslab, dhdr, dcoords, dsidx, pout, dkeys, ks, n_out, off, oM, oK, oq, op};
                 k_rows<<<nsm * 8, 256>>>(R); ++launches;
                 CK(cudaGetLastError());
             }

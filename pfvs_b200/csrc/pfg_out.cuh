@@ -125,16 +125,28 @@ __device__ __forceinline__ int64_t row_entry(const int64_t *T, const int32_t *c,
     return s;
 }
 
+// warp per kept point: its M row into the keys (lanes own entries)
 __global__ void k_keys(OutArgs O, unsigned long long n_kept)
 {
-    for (unsigned long long t = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; t < n_kept;
-         t += (unsigned long long)gridDim.x * blockDim.x) {
+    const int lane = threadIdx.x & 31;
+    const unsigned long long w = (blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x) >> 5;
+    const unsigned long long nw = ((unsigned long long)gridDim.x * blockDim.x) >> 5;
+    for (unsigned long long t = w; t < n_kept; t += nw) {
         const unsigned k = O.idx[t];
         const Dir D = O.dirs[O.hdr[k].pid];
-        const int64_t *BT = O.slab + D.slab + slab_layout(D.h, D.d).bt;
+        const int h = D.h, d = D.d;
+        const int64_t *BT = O.slab + D.slab + slab_layout(h, d).bt;
         const int32_t *c = O.coords + (unsigned long long)k * MD;
+        const int32_t c0 = lane < d ? c[lane] : 0, c1 = lane + 32 < d ? c[lane + 32] : 0;
+        int64_t m0 = 0, m1 = 0;
+        for (int a = 0; a < d; ++a) {
+            const int64_t ca = __shfl_sync(FULL, a < 32 ? c0 : c1, a & 31);
+            if (lane < h) m0 += (int64_t)(int32_t)BT[a * h + lane] * ca;
+            if (lane + 32 < h) m1 += (int64_t)(int32_t)BT[a * h + lane + 32] * ca;
+        }
         int64_t *key = O.keys + t * O.ks;
-        for (int r = 0; r < D.h; ++r) key[r] = row_entry(BT, c, D.d, D.h, r);
+        if (lane < h) key[lane] = m0;
+        if (lane + 32 < h) key[lane + 32] = m1;
     }
 }
 
@@ -242,14 +254,16 @@ __global__ void k_merge(OutArgs O, unsigned long long n_kept, unsigned L, const 
     }
 }
 
-// sorted segment-local positions -> point indices in output order
-__global__ void k_order(OutArgs O, unsigned long long n_kept, const unsigned *perm, unsigned *out_idx)
+// sorted segment-local positions -> point indices (and key rows) in output order
+__global__ void k_order(OutArgs O, unsigned long long n_kept, const unsigned *perm, unsigned *out_idx,
+                        unsigned *out_key)
 {
     for (unsigned long long t = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; t < n_kept;
          t += (unsigned long long)gridDim.x * blockDim.x) {
         const int pid = O.hdr[O.idx[t]].pid;
         const unsigned long long s0 = O.seg[pid];
         out_idx[t] = O.idx[s0 + perm[t]];
+        out_key[t] = (unsigned)(s0 + perm[t]);
     }
 }
 
@@ -259,6 +273,9 @@ struct RowArgs {
     const PointHdr *hdr;
     const int32_t *coords;
     const unsigned *idx;          // points in output order
+    const unsigned *krow;         // their rows of keys (the M rows)
+    const int64_t *keys;
+    int ks;
     unsigned long long n_out;
     int64_t pid_base;
     int64_t *M, *Kn, *q, *pidx;   // output (n_out, MH), (n_out,)
@@ -276,20 +293,16 @@ __global__ void k_rows(RowArgs R)
         const Dir D = R.dirs[P.pid];
         const int h = D.h, d = D.d;
         const Slab L = slab_layout(h, d);
-        const int64_t *BT = R.slab + D.slab + L.bt, *ZT = R.slab + D.slab + L.zt;
+        const int64_t *ZT = R.slab + D.slab + L.zt;
         const int32_t *c = R.coords + (unsigned long long)k * MD;
         const int32_t c0 = lane < d ? c[lane] : 0, c1 = lane + 32 < d ? c[lane + 32] : 0;
-        int64_t m0 = 0, m1 = 0, k0 = 0, k1 = 0;
+        const int64_t *key = R.keys + (unsigned long long)R.krow[t] * R.ks;
+        const int64_t m0 = lane < h ? key[lane] : 0, m1 = lane + 32 < h ? key[lane + 32] : 0;
+        int64_t k0 = 0, k1 = 0;
         for (int a = 0; a < d; ++a) {
             const int64_t ca = __shfl_sync(FULL, a < 32 ? c0 : c1, a & 31);
-            if (lane < h) {
-                m0 += (int64_t)(int32_t)BT[a * h + lane] * ca;
-                k0 += (int64_t)(int32_t)ZT[a * h + lane] * ca;
-            }
-            if (lane + 32 < h) {
-                m1 += (int64_t)(int32_t)BT[a * h + lane + 32] * ca;
-                k1 += (int64_t)(int32_t)ZT[a * h + lane + 32] * ca;
-            }
+            if (lane < h) k0 += (int64_t)(int32_t)ZT[a * h + lane] * ca;
+            if (lane + 32 < h) k1 += (int64_t)(int32_t)ZT[a * h + lane + 32] * ca;
         }
         int64_t *Mr = R.M + t * MH, *Kr = R.Kn + t * MH;
         Mr[lane] = m0; Mr[lane + 32] = m1;

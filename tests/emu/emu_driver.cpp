@@ -131,8 +131,8 @@ extern "C" int emu_coni_batch(const pfg_input *in, int precision, int n_warps, p
             launch(4, [&] { k_merge(O, n_out, (unsigned)L, pin, pout); });
             std::swap(pin, pout);
         }
-        launch(4, [&] { k_order(O, n_out, pin, sidx.data()); });
-        RowArgs R{dirs.data(), slab.data(), hdr.data(), coords.data(), sidx.data(), n_out, 0,
+        launch(4, [&] { k_order(O, n_out, pin, sidx.data(), pout); });
+        RowArgs R{dirs.data(), slab.data(), hdr.data(), coords.data(), sidx.data(), pout, keys.data(), ks, n_out, 0,
                   out->M, out->Kn, out->q, out->pidx};
         launch(4, [&] { k_rows(R); });
     }
