@@ -46,15 +46,23 @@ PFG_HD bool sub_ovf(i128 a, i128 b, i128 *r)
     *r = s;
     return ((a >= 0) != (b >= 0)) && ((s >= 0) != (a >= 0));
 }
-// a * b with overflow detection
+// a * b with overflow detection: true iff |a b| > 2^127 - 1.  The magnitude
+// product is formed from 64-bit limbs (no 128-bit division): when both
+// magnitudes reach 2^64 it is at least 2^128; otherwise one factor x is below
+// 2^64 and |a b| = hi(u) x 2^64 + lo(u) x for the other factor u.
 PFG_HD bool mul_ovf(i128 a, i128 b, i128 *r)
 {
     u128 ua = uabs(a), ub = uabs(b);
     const u128 lim = (u128)1 << 63;
     if (ua < lim && ub < lim) { *r = a * b; return false; }
-    if (ua == 0 || ub == 0) { *r = 0; return false; }
-    if (ub > ((((u128)1) << 127) - 1) / ua) return true;
-    u128 m = ua * ub;
+    if ((uint64_t)(ua >> 64) && (uint64_t)(ub >> 64)) return true;
+    if (ub >> 64) { u128 t = ua; ua = ub; ub = t; }
+    const uint64_t x = (uint64_t)ub;
+    const u128 p0 = (u128)(uint64_t)ua * x, p1 = (u128)(uint64_t)(ua >> 64) * x;
+    if ((uint64_t)(p1 >> 64)) return true;
+    const u128 hi = (p0 >> 64) + (u128)(uint64_t)p1;
+    if (hi >> 63) return true;
+    const u128 m = (hi << 64) | (u128)(uint64_t)p0;
     *r = ((a < 0) != (b < 0)) ? -(i128)m : (i128)m;
     return false;
 }

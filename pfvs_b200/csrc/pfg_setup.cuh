@@ -89,7 +89,10 @@ struct SetupArgs {
 // Per-stage cycle accounting of the setup, compiled in only with
 // -DPFG_STAGE_CLOCKS (a profiling build): lane 0 adds the clock64() cycles
 // spent in each stage to pfg_stage_cycles[stage & 31]; counters [32..34]
-// count LLL calls, swaps and size-reduction passes.
+// count LLL calls, swaps and size-reduction passes with non-zero
+// multipliers, [40..43] the cycles in the LLL's Gram-Schmidt rows, Babai
+// loops, exact updates and swaps, [44..45] the Gram-Schmidt rows and Babai
+// loops run.
 #ifdef PFG_STAGE_CLOCKS
 __device__ unsigned long long pfg_stage_cycles[64];
 struct StageClock {
@@ -116,6 +119,8 @@ struct StageClock {
     __device__ ~StageClock() { mark(stage); }
 };
 #define PFG_COUNT(i, v) do { if ((threadIdx.x & 31) == 0) atomicAdd(&pfg_stage_cycles[32 + (i)], (unsigned long long)(v)); } while (0)
+#define PFG_T0(t) const long long t = clock64()
+#define PFG_TACC(i, t) PFG_COUNT(i, clock64() - (t))
 #else
 struct StageClock {
     int &stage;
@@ -123,6 +128,8 @@ struct StageClock {
     __device__ void mark(int s) { stage = s; }
 };
 #define PFG_COUNT(i, v) do { } while (0)
+#define PFG_T0(t) do { } while (0)
+#define PFG_TACC(i, t) do { } while (0)
 #endif
 
 __device__ __forceinline__ double warp_sum(double x)
@@ -166,28 +173,41 @@ template <int N> struct Lll {
 
 // mu(k, j) (j < k) and bb[k] from G(k, .) and the rows above: r_j = mu_kj
 // bb_j solves the unit lower-triangular system r_j = G_kj - sum_{l<j} mu_jl
-// r_l (forward substitution by columns, lanes own rows).
+// r_l (forward substitution by columns, lanes own rows); afterwards lane l
+// holds r_l, so mu_kl = r_l / bb_l and bb_k = G_kk - sum_l mu_kl r_l are
+// formed in parallel.
 template <int N> PFG_NOINLINE __device__ void lll_gs(LllMem<N> *S, int k, int lane)
 {
+    PFG_T0(t_gs);
+    PFG_COUNT(12, 1);
     double a0 = lane < k ? (double)S->G[gix(k, lane)] : 0.0;
     double a1 = 0.0;
     if (N > 32) a1 = lane + 32 < k ? (double)S->G[gix(k, lane + 32)] : 0.0;
-    double s = 0.0;
-    double *muk = S->mu + mix(k, 0);
-    for (int j = 0; j < k; ++j) {
+    for (int j = 0; j < k - 1; ++j) {
         const double rj = __shfl_sync(FULL, (N > 32 && j >= 32) ? a1 : a0, j & 31);
-        const double mkj = rj * S->ibb[j];
-        s = fma(mkj, rj, s);
-        if (lane == (j & 31)) muk[j] = mkj;
         if (lane > j && lane < k) a0 = fma(-S->mu[mix(lane, j)], rj, a0);
         if (N > 32 && lane + 32 > j && lane + 32 < k) a1 = fma(-S->mu[mix(lane + 32, j)], rj, a1);
     }
+    double *muk = S->mu + mix(k, 0);
+    double s = 0.0;
+    if (lane < k) {
+        const double m = a0 * S->ibb[lane];
+        muk[lane] = m;
+        s = m * a0;
+    }
+    if (N > 32 && lane + 32 < k) {
+        const double m = a1 * S->ibb[lane + 32];
+        muk[lane + 32] = m;
+        s = fma(m, a1, s);
+    }
+    s = warp_sum(s);
     if (lane == 0) {
         const double b = (double)S->G[gix(k, k)] - s;
         S->bb[k] = b;
         S->ibb[k] = 1.0 / b;
     }
     __syncwarp();
+    PFG_TACC(8, t_gs);
 }
 
 // Size-reduce row k against rows 0..k-1: the multipliers q_j come from the
@@ -198,23 +218,42 @@ template <int N> PFG_NOINLINE __device__ int lll_reduce(Lll<N> &L, int k, int la
 {
     LllMem<N> *S = L.S;
     for (int pass = 0; pass < 16; ++pass) {
+        PFG_T0(t_q);
+        PFG_COUNT(13, 1);
         double r0 = lane < k ? S->mu[mix(k, lane)] : 0.0;
         double r1 = 0.0;
         if (N > 32) r1 = lane + 32 < k ? S->mu[mix(k, lane + 32)] : 0.0;
+        // Babai from j = k-1 down: q_j = rint(x_j) of the running coefficient,
+        // which is 0 exactly when |x_j| <= 1/2; so only the rows whose running
+        // coefficient is outside [-1/2, 1/2] (or NaN, which fails the range
+        // check) are visited, highest first, found by ballot.
         uint64_t qmask = 0;                             // rows j with q_j != 0 (uniform)
-        for (int j = k - 1; j >= 0; --j) {
+        int64_t q0 = 0, q1 = 0;                         // q_lane, q_{lane+32}
+        int top = k;
+        for (;;) {
+            uint64_t cand = __ballot_sync(FULL, lane < top && !(fabs(r0) <= 0.5));
+            if (N > 32) cand |= (uint64_t)__ballot_sync(FULL, lane + 32 < top && !(fabs(r1) <= 0.5)) << 32;
+            if (!cand) break;
+            const int j = 63 - __clzll((long long)cand);
             const double x = __shfl_sync(FULL, (N > 32 && j >= 32) ? r1 : r0, j & 31);
             const double qd = rint(x);
             PFG_UNIFORM(qd);
             if (!(fabs(qd) <= 9.0e18)) return ST_OVERFLOW;
-            if (lane == 0) S->q[j] = (int64_t)qd;
-            if (qd == 0.0) continue;
             qmask |= 1ull << j;
+            if (lane == (j & 31)) {
+                if (N > 32 && j >= 32) q1 = (int64_t)qd;
+                else q0 = (int64_t)qd;
+            }
             if (lane < j) r0 = fma(-qd, S->mu[mix(j, lane)], r0);
             if (N > 32 && lane + 32 < j) r1 = fma(-qd, S->mu[mix(j, lane + 32)], r1);
+            top = j;
         }
+        PFG_TACC(9, t_q);
         if (!qmask) return 0;
         PFG_COUNT(2, 1);
+        PFG_T0(t_u);
+        if (lane < k) S->q[lane] = q0;
+        if (N > 32 && lane + 32 < k) S->q[lane + 32] = q1;
         __syncwarp();                                   // q[] visible to all lanes
         bool bad = false;
         // new row k of B (lanes own columns)
@@ -276,6 +315,7 @@ template <int N> PFG_NOINLINE __device__ int lll_reduce(Lll<N> &L, int k, int la
         if (N > 32 && l1 < L.M && l1 != k) S->G[gix(k, l1)] = g1;
         if (lane == 0) S->G[gix(k, k)] = gkk;
         __syncwarp();
+        PFG_TACC(10, t_u);
         lll_gs(S, k, lane);
     }
     return 0;
@@ -306,13 +346,15 @@ template <int N> PFG_NOINLINE __device__ void lll_swap(Lll<N> &L, int k, int lan
         const i128 t = S->G[gix(k, k)];
         S->G[gix(k, k)] = S->G[gix(k - 1, k - 1)];
         S->G[gix(k - 1, k - 1)] = t;
+        // one division: 1/bb'_k = Bn / (b1 b2) from the old inverses
         const double m = S->mu[mix(k, k - 1)], b1 = S->bb[k - 1], b2 = S->bb[k];
         const double Bn = k == 1 ? (double)S->G[0] : fma(m * m, b1, b2);
-        S->mu[mix(k, k - 1)] = m * b1 / Bn;
-        S->bb[k] = b1 * b2 / Bn;
+        const double iBn = 1.0 / Bn;
+        S->mu[mix(k, k - 1)] = m * b1 * iBn;
+        S->bb[k] = b1 * b2 * iBn;
         S->bb[k - 1] = Bn;
-        S->ibb[k] = 1.0 / S->bb[k];
-        S->ibb[k - 1] = 1.0 / Bn;
+        S->ibb[k] = Bn * S->ibb[k - 1] * S->ibb[k];
+        S->ibb[k - 1] = iBn;
     }
     __syncwarp();
 }
@@ -337,7 +379,9 @@ template <int N> PFG_NOINLINE __device__ int warp_lll(Lll<N> &L, int m, bool has
         __syncwarp();                       // (every lane has read them before lll_swap writes)
         if (!(bk > 0)) return ST_OVERFLOW;
         if (bk < (delta - mk * mk) * bk1) {
+            PFG_T0(t_s);
             lll_swap(L, k, lane);
+            PFG_TACC(11, t_s);
             PFG_COUNT(1, 1);
             if (k > 1) --k;
         } else {
