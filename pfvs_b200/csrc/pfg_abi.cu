@@ -7,11 +7,14 @@
 //   k_count .. k_rows      canonical output rows              (pfg_out.cuh)
 //   k_pfv_count .. k_pfv_rows   points -> PFVs (pfg_coni_pfvs)  (pfg_pfv.cuh)
 // with one host synchronisation at the end of a batch (point count, output
-// size).  No CPU fallback: a direction the device cannot finish exactly is
-// reported with a negative status.
+// size).  The point rows of a batch go to the caller's pinned block on a
+// second (copy) stream, overlapping the next batch when there are several.  No CPU fallback: a
+// direction the device cannot finish exactly is reported with a negative
+// status.
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cstdarg>
 #include <cstdio>
 #include <cstdlib>
@@ -55,7 +58,7 @@ enum {
     W_GEO, W_KAPPA, W_MB, W_PS, W_PGEO, W_SLABOFF, W_SLAB, W_DIRS, W_SCRATCH, W_TODO32, W_TODOALL, W_ORDER,
     W_CTL, W_ITEMS, W_READY, W_HDR, W_COORDS, W_DIRNODES, W_DIRPASS,
     W_KEYS, W_COUNT, W_FILL, W_SEG, W_IDX, W_CSEG, W_SUM, W_PERM, W_PERM2, W_SIDX, W_PCNT, W_PKG, W_PEPT, W_PEG, W_PEK0, W_PEORD, W_PNONS, W_PKEEP,
-    W_PERR, W_PSORT, W_PK, W_PM, W_PP, W_PRIMES, W_OM, W_OK, W_OQ, W_OP, W_RETRY, W_N
+    W_PERR, W_PSORT, W_PK, W_PM, W_PP, W_PRIMES, W_OM, W_OK, W_OQ, W_OP, W_OM2, W_OK2, W_OQ2, W_OP2, W_RETRY, W_N
 };
 
 struct Workspace {
@@ -63,6 +66,10 @@ struct Workspace {
     void *p[W_N] = {};
     size_t cap[W_N] = {};
     unsigned long long pts_cap = 1ull << 20;    // point buffer: grows to the largest batch seen
+    double rows_per_dir = 0.0;                  // output rows per direction of the last call
+    cudaStream_t copy = nullptr;                // device-to-host row copies (non-blocking)
+    cudaEvent_t rows_done[2] = {}, copied[2] = {};  // per output slot: rows written / copied out
+    bool copy_pending[2] = {false, false};
 };
 
 std::mutex g_ws_mu;
@@ -177,13 +184,27 @@ void pinned_release_idle()
     for (auto &e : idle) cudaFreeHost(e.second);
 }
 
-struct Chunk { int64_t *M, *Kn, *q, *pidx; size_t n; };
-
-void chunk_free(Chunk &c)
-{
-    for (int64_t *p : {c.M, c.Kn, c.q, c.pidx}) pinned_put(p);
-    c = Chunk{nullptr, nullptr, nullptr, nullptr, 0};
-}
+// The caller's point rows: one pinned block per array, filled batch by batch
+// by asynchronous copies on the workspace's copy stream.
+struct RowSink {
+    int64_t *M = nullptr, *Kn = nullptr, *q = nullptr, *pidx = nullptr;
+    size_t n = 0, cap = 0;
+    bool alloc(size_t rows)
+    {
+        M = (int64_t *)pinned_get(rows * MH * 8);
+        Kn = (int64_t *)pinned_get(rows * MH * 8);
+        q = (int64_t *)pinned_get(rows * 8);
+        pidx = (int64_t *)pinned_get(rows * 8);
+        cap = rows;
+        return M && Kn && q && pidx;
+    }
+    void release()
+    {
+        for (int64_t *p : {M, Kn, q, pidx}) pinned_put(p);
+        M = Kn = q = pidx = nullptr;
+        n = cap = 0;
+    }
+};
 
 // PFVs of a pfg_coni_pfvs call, per batch
 struct PfvChunk { int64_t *K, *M, *pidx; size_t n; };
@@ -336,7 +357,12 @@ static int coni_run(const pfg_input *in, const pfg_options *opt_in, pfg_output *
     int64_t launches = 0;
     Workspace &W = workspace(in->device);
     std::unique_lock<std::mutex> lock(W.mu);
-    std::vector<Chunk> chunks;
+    RowSink rows;
+    int sub = 0;                                // batches done (output slot = sub & 1)
+    const auto t_call = std::chrono::steady_clock::now();
+    auto host_ms = [&]() {                      // host wall time since the call began (verbose)
+        return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_call).count();
+    };
     cudaEvent_t ev[8] = {};
     int64_t koff_total = 0, moff_total = 0;
     Geo *dgeo = nullptr;
@@ -347,6 +373,13 @@ static int coni_run(const pfg_input *in, const pfg_options *opt_in, pfg_output *
     CK(cudaSetDevice(in->device));
     CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, in->device));
     for (auto &e : ev) CK(cudaEventCreate(&e));
+    if (!W.copy) {
+        CK(cudaStreamCreateWithFlags(&W.copy, cudaStreamNonBlocking));
+        for (int k = 0; k < 2; ++k) {
+            CK(cudaEventCreateWithFlags(&W.rows_done[k], cudaEventDisableTiming));
+            CK(cudaEventCreateWithFlags(&W.copied[k], cudaEventDisableTiming));
+        }
+    }
     WS(dgeo, W_GEO, geos.size() * sizeof(Geo));
     WS(dkappa, W_KAPPA, koff_total * 8);
     WS(dmb, W_MB, moff_total * 8);
@@ -517,7 +550,9 @@ static int coni_run(const pfg_input *in, const pfg_options *opt_in, pfg_output *
             }
             CK(cudaEventRecord(ev[2]));
             SearchCtl hctl[2];
+            if (in->verbose) fprintf(stderr, "pfg: [%.1f ms] batch @%lld: launched through the search\n", host_ms(), (long long)off);
             CK(cudaMemcpy(hctl, dctl, 2 * sizeof(SearchCtl), cudaMemcpyDeviceToHost));
+            if (in->verbose) fprintf(stderr, "pfg: [%.1f ms] search done\n", host_ms());
             if (hctl[0].err || hctl[1].err) {
                 set_err(out, "search: a bounded device wait ran out (status %d)", hctl[0].err ? hctl[0].err : hctl[1].err);
                 rc = 1;
@@ -563,11 +598,17 @@ static int coni_run(const pfg_input *in, const pfg_options *opt_in, pfg_output *
             unsigned long long summary[3] = {0, 0, 0};
             CK(cudaMemcpy(summary, dsum, sizeof summary, cudaMemcpyDeviceToHost));
             const unsigned long long n_out = summary[0], n_chunks = summary[1], longest = summary[2];
+            // output slot of this batch: free once the copy of the batch before last is done
+            const int slot = sub & 1;
+            if (W.copy_pending[slot]) {
+                CK(cudaEventSynchronize(W.copied[slot]));
+                W.copy_pending[slot] = false;
+            }
             int64_t *oM, *oK, *oq, *op;
-            WS(oM, W_OM, std::max<unsigned long long>(n_out, 1) * MH * 8);
-            WS(oK, W_OK, std::max<unsigned long long>(n_out, 1) * MH * 8);
-            WS(oq, W_OQ, std::max<unsigned long long>(n_out, 1) * 8);
-            WS(op, W_OP, std::max<unsigned long long>(n_out, 1) * 8);
+            WS(oM, slot ? W_OM2 : W_OM, std::max<unsigned long long>(n_out, 1) * MH * 8);
+            WS(oK, slot ? W_OK2 : W_OK, std::max<unsigned long long>(n_out, 1) * MH * 8);
+            WS(oq, slot ? W_OQ2 : W_OQ, std::max<unsigned long long>(n_out, 1) * 8);
+            WS(op, slot ? W_OP2 : W_OP, std::max<unsigned long long>(n_out, 1) * 8);
             if (n_out) {
                 const int smem_sort = SORT_CAP * KEYN * 8 + SORT_CAP * 4;
                 CK(cudaFuncSetAttribute(k_segsort, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_sort));
@@ -648,14 +689,34 @@ static int coni_run(const pfg_input *in, const pfg_options *opt_in, pfg_output *
             }
             CK(cudaEventRecord(ev[4]));
             if (n_out && !pfv) {
-                Chunk c{(int64_t *)pinned_get(n_out * MH * 8), (int64_t *)pinned_get(n_out * MH * 8),
-                        (int64_t *)pinned_get(n_out * 8), (int64_t *)pinned_get(n_out * 8), (size_t)n_out};
-                chunks.push_back(c);
-                if (!c.M || !c.Kn || !c.q || !c.pidx) { set_err(out, "out of pinned host memory"); rc = 1; goto fail; }
-                CK(cudaMemcpy(c.M, oM, n_out * MH * 8, cudaMemcpyDeviceToHost));
-                CK(cudaMemcpy(c.Kn, oK, n_out * MH * 8, cudaMemcpyDeviceToHost));
-                CK(cudaMemcpy(c.q, oq, n_out * 8, cudaMemcpyDeviceToHost));
-                CK(cudaMemcpy(c.pidx, op, n_out * 8, cudaMemcpyDeviceToHost));
+                if (rows.n + n_out > rows.cap) {
+                    // room for the whole call, from this batch's (or the last call's) rows per direction
+                    const double per = std::max((double)n_out / nb, W.rows_per_dir);
+                    const size_t cap = std::max<size_t>(rows.n + n_out, (size_t)(per * (double)NP * 1.1) + 4096);
+                    RowSink bigger;
+                    if (!bigger.alloc(cap)) { bigger.release(); set_err(out, "out of pinned host memory"); rc = 1; goto fail; }
+                    if (rows.n) {
+                        CK(cudaStreamSynchronize(W.copy));
+                        memcpy(bigger.M, rows.M, rows.n * MH * 8);
+                        memcpy(bigger.Kn, rows.Kn, rows.n * MH * 8);
+                        memcpy(bigger.q, rows.q, rows.n * 8);
+                        memcpy(bigger.pidx, rows.pidx, rows.n * 8);
+                        bigger.n = rows.n;
+                    }
+                    rows.release();
+                    rows = bigger;
+                }
+                CK(cudaEventRecord(W.rows_done[slot], 0));
+                CK(cudaStreamWaitEvent(W.copy, W.rows_done[slot], 0));
+                CK(cudaMemcpyAsync(rows.M + rows.n * MH, oM, n_out * MH * 8, cudaMemcpyDeviceToHost, W.copy));
+                CK(cudaMemcpyAsync(rows.Kn + rows.n * MH, oK, n_out * MH * 8, cudaMemcpyDeviceToHost, W.copy));
+                CK(cudaMemcpyAsync(rows.q + rows.n, oq, n_out * 8, cudaMemcpyDeviceToHost, W.copy));
+                CK(cudaMemcpyAsync(rows.pidx + rows.n, op, n_out * 8, cudaMemcpyDeviceToHost, W.copy));
+                CK(cudaEventRecord(W.copied[slot], W.copy));
+                W.copy_pending[slot] = true;
+                rows.n += n_out;
+                if (in->verbose) fprintf(stderr, "pfg: [%.1f ms] rows %llu queued for copy (block of %zu rows)\n",
+                                         host_ms(), n_out, rows.cap);
             }
             // statuses
             {
@@ -702,35 +763,23 @@ static int coni_run(const pfg_input *in, const pfg_options *opt_in, pfg_output *
                             hctl[0].donated + hctl[1].donated, retries);
             }
             off += nb;
+            ++sub;
         }
     }
-    {
-        size_t n = 0;
-        for (auto &c : chunks) n += c.n;
-        out->n = (int64_t)n;
-        if (chunks.size() == 1) {
-            out->M = chunks[0].M; out->Kn = chunks[0].Kn; out->q = chunks[0].q; out->pidx = chunks[0].pidx;
-            chunks.clear();
-        } else {
-            out->M = (int64_t *)pinned_get(n * MH * 8);
-            out->Kn = (int64_t *)pinned_get(n * MH * 8);
-            out->q = (int64_t *)pinned_get(n * 8);
-            out->pidx = (int64_t *)pinned_get(n * 8);
-            if (!out->M || !out->Kn || !out->q || !out->pidx) { set_err(out, "out of pinned host memory"); rc = 1; goto fail; }
-            size_t base = 0;
-            for (auto &c : chunks) {
-                memcpy(out->M + base * MH, c.M, c.n * MH * 8);
-                memcpy(out->Kn + base * MH, c.Kn, c.n * MH * 8);
-                memcpy(out->q + base, c.q, c.n * 8);
-                memcpy(out->pidx + base, c.pidx, c.n * 8);
-                base += c.n;
-                chunk_free(c);
-            }
-            chunks.clear();
-        }
-    }
+    if (in->verbose) fprintf(stderr, "pfg: [%.1f ms] all batches done\n", host_ms());
+    CK(cudaStreamSynchronize(W.copy));
+    if (in->verbose) fprintf(stderr, "pfg: [%.1f ms] copies done\n", host_ms());
+    W.copy_pending[0] = W.copy_pending[1] = false;
+    out->n = (int64_t)rows.n;
+    out->M = rows.M; out->Kn = rows.Kn; out->q = rows.q; out->pidx = rows.pidx;
+    if (!pfv) W.rows_per_dir = NP ? (double)rows.n / (double)NP : 0.0;
+    rows = RowSink();
 fail:
-    for (auto &c : chunks) chunk_free(c);
+    if (W.copy) {
+        cudaStreamSynchronize(W.copy);          // no copy may still write into a block released below
+        W.copy_pending[0] = W.copy_pending[1] = false;
+    }
+    rows.release();
     for (auto &e : ev) if (e) cudaEventDestroy(e);
     if (rc) {
         cudaGetLastError();

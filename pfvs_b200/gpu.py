@@ -174,31 +174,38 @@ def _pack(geoms, ps, pgeo, MH):
     n_p = len(pgeo)
     if n_p and (np.any(pgeo < 0) or np.any(pgeo >= n_geo)):
         raise ValueError("pgeo: geometry index out of range")
-    P = np.zeros((max(n_p, 1), MH), dtype=np.int64)
     if isinstance(ps, np.ndarray) and ps.ndim == 2:
         W = ps.shape[1]
         if W > MH:
             raise ValueError("a p-vector is longer than its geometry's h11")
-        P[:n_p, :W] = ps
-        hp = h[pgeo] if n_p else h[:0]
-        for hv in np.unique(hp[hp < W]) if n_p else ():     # entries beyond h11 must be 0
-            rows = np.flatnonzero(hp == hv)
-            if np.any(P[rows, hv:W]):
+        if ps.shape[0] != n_p:
+            raise ValueError("ps and pgeo differ in length")
+        if n_p:
+            hp = h[pgeo]
+            if W > hp.min():                                  # entries beyond h11 must be 0
+                if np.any((ps != 0) & (np.arange(W)[None, :] >= hp[:, None])):
+                    raise ValueError("a p-vector is longer than its geometry's h11")
+        if n_p and W == MH and ps.dtype == np.int64 and ps.flags.c_contiguous:
+            P = ps                                            # already the library's layout
+        else:
+            P = np.zeros((max(n_p, 1), MH), dtype=np.int64)
+            P[:n_p, :W] = ps
+    else:
+        P = np.zeros((max(n_p, 1), MH), dtype=np.int64)
+        if n_p:
+            # one flat copy and one scatter (a list of 1-d arrays)
+            lens = np.fromiter((len(p) for p in ps), dtype=np.int64, count=n_p)
+            if lens.max() > MH:
                 raise ValueError("a p-vector is longer than its geometry's h11")
-    elif n_p:
-        # one flat copy and one scatter (a list of 1-d arrays)
-        lens = np.fromiter((len(p) for p in ps), dtype=np.int64, count=n_p)
-        if lens.max() > MH:
-            raise ValueError("a p-vector is longer than its geometry's h11")
-        flat = np.concatenate([np.asarray(p, dtype=np.int64).ravel() for p in ps])
-        rows = np.repeat(np.arange(n_p), lens)
-        cols = np.arange(len(flat)) - np.repeat(np.cumsum(lens) - lens, lens)
-        P[rows, cols] = flat
-        long_rows = np.flatnonzero(lens > h[pgeo])
-        if len(long_rows):
-            hh = h[pgeo[long_rows]]
-            if np.any(P[long_rows][np.arange(MH)[None, :] >= hh[:, None]] != 0):
-                raise ValueError("a p-vector is longer than its geometry's h11")
+            flat = np.concatenate([np.asarray(p, dtype=np.int64).ravel() for p in ps])
+            rows = np.repeat(np.arange(n_p), lens)
+            cols = np.arange(len(flat)) - np.repeat(np.cumsum(lens) - lens, lens)
+            P[rows, cols] = flat
+            long_rows = np.flatnonzero(lens > h[pgeo])
+            if len(long_rows):
+                hh = h[pgeo[long_rows]]
+                if np.any(P[long_rows][np.arange(MH)[None, :] >= hh[:, None]] != 0):
+                    raise ValueError("a p-vector is longer than its geometry's h11")
     return h, Q, qmax, linmin, kap, Mb, P, pgeo, n_p
 
 

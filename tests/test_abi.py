@@ -38,3 +38,38 @@ def test_struct_layouts_match_reference_ctypes():
         "device", "batch", "verbose"]
     assert [f for f, _ in gpu._Output._fields_] == [
         "n", "M", "Kn", "q", "pidx", "pstat", "seconds_gpu", "err"]
+
+
+def test_input_packing_forms_agree_and_validate():
+    """The p-vector forms the host accepts (a list of 1-d arrays, a narrow or
+    full-width 2-d array) pack to the same (n_p, pfg_max_h11()) block; a
+    full-width C-contiguous int64 array is used in place; entries beyond a
+    geometry's h11 and a length mismatch with pgeo are rejected."""
+    import numpy as np
+    import pytest
+    from pfvs_b200 import gpu, workloads
+    from parity import layout
+    geoms, ps, pgeo, _ = layout(workloads.build("mixed", n_p=64))
+    MH = 64
+    P_list = gpu._pack(geoms, ps, pgeo, MH)[6]
+    W = max(len(p) for p in ps)
+    narrow = np.zeros((len(ps), W), np.int64)
+    for i, p in enumerate(ps):
+        narrow[i, :len(p)] = p
+    full = np.zeros((len(ps), MH), np.int64)
+    full[:, :W] = narrow
+    np.testing.assert_array_equal(gpu._pack(geoms, narrow, pgeo, MH)[6], P_list)
+    P_full = gpu._pack(geoms, full, pgeo, MH)[6]
+    assert P_full is full
+    np.testing.assert_array_equal(P_full, P_list)
+    h0 = np.asarray(geoms[int(pgeo[0])]["kappa"]).shape[0]
+    for bad in (full.copy(), narrow.copy()):
+        bad[0, h0] = 1
+        with pytest.raises(ValueError):
+            gpu._pack(geoms, bad, pgeo, MH)
+    bad_list = [np.asarray(p) for p in ps]
+    bad_list[0] = np.concatenate([bad_list[0], [0] * (h0 - len(bad_list[0])), [1]])
+    with pytest.raises(ValueError):
+        gpu._pack(geoms, bad_list, pgeo, MH)
+    with pytest.raises(ValueError):
+        gpu._pack(geoms, full[:-1], pgeo, MH)

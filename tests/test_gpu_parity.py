@@ -124,3 +124,17 @@ def test_output_canonical_on_a_large_batch():
     assert _is_canonical(M, Kn, pidx)
     b = gpu.coni_batch_multi_ex(geoms, ps, pgeo, precision=gpu.PREC_FP64)
     assert_same(b, a)
+
+
+def test_batch_splits_give_identical_rows():
+    """The rows do not depend on how the directions are split into batches:
+    one batch (explicit and default) and six batches (both device output
+    slots reused, each batch's rows copied out while the next computes)."""
+    w = workloads.build("mixed", n_p=16384)
+    geoms, ps, pgeo, _ = layout(w)
+    one = gpu.coni_batch_multi_ex(geoms, ps, pgeo, batch=len(ps))
+    for b in (0, 3000):
+        x = gpu.coni_batch_multi_ex(geoms, ps, pgeo, batch=b)
+        assert_same(x, one)
+        np.testing.assert_array_equal(x[4], one[4])
+        assert x[6]["nodes"] == one[6]["nodes"]
