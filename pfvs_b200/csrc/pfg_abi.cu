@@ -1,6 +1,7 @@
 // libpfvs_gpu.so: host side of the batched coni pipeline and its C ABI
 // (include/pfvs_gpu.h).  Per batch of directions, on one stream:
-//   k_setup      lattice setup, one warp per direction   (pfg_setup.cuh)
+//   k_setup<.,0..2>  lattice setup in three phase kernels, one warp per
+//                direction                                 (pfg_setup.cuh)
 //   k_search<f>  FP32-pruned persistent search            (pfg_search.cuh)
 //   k_flip       FP32 successes -> done; -11 -> FP64 retry
 //   k_search<d>  FP64-pruned search of the rest
@@ -430,9 +431,11 @@ static int coni_run(const pfg_input *in, const pfg_options *opt_in, pfg_output *
             const size_t smem32 = sizeof(LllMem<32>);
             int grid32 = 0, grid64 = 0;
             if (n32) {
-                CK(cudaFuncSetAttribute(k_setup<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem32));
+                CK(cudaFuncSetAttribute(k_setup<32, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem32));
+                CK(cudaFuncSetAttribute(k_setup<32, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem32));
+                CK(cudaFuncSetAttribute(k_setup<32, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem32));
                 int bpsm = 0;
-                CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bpsm, k_setup<32>, 32, smem32));
+                CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bpsm, k_setup<32, 1>, 32, smem32));
                 grid32 = std::min(n32, nsm * std::max(1, bpsm));
             }
             if (n64) grid64 = std::min((n64 + 3) / 4, nsm * 2);
@@ -472,18 +475,20 @@ static int coni_run(const pfg_input *in, const pfg_options *opt_in, pfg_output *
             CK(cudaEventRecord(ev[0]));
             {
                 unsigned *counters = (unsigned *)((char *)dctl + 2 * sizeof(SearchCtl));
-                if (n32) {
-                    SetupArgs SA{dgeo, dkappa, dmb, dps, dpgeo, dslaboff, dslab, ddirs, dscr, n32,
-                                 counters, dorder, 1, gcd_min_tree};
-                    k_setup<32><<<grid32, 32, smem32>>>(SA); ++launches;
-                    CK(cudaGetLastError());
-                }
-                if (n64) {
-                    SetupArgs SA{dgeo, dkappa, dmb, dps, dpgeo, dslaboff, dslab, ddirs, dscr, n64,
-                                 counters + 1, dorder + n32, 0, gcd_min_tree};
-                    k_setup<MH><<<grid64, 128>>>(SA); ++launches;
-                    CK(cudaGetLastError());
-                }
+                // phases in order, each over all directions (one work counter per launch)
+                SetupArgs SA32{dgeo, dkappa, dmb, dps, dpgeo, dslaboff, dslab, ddirs, dscr, n32,
+                               counters, dorder, 1, gcd_min_tree};
+                SetupArgs SA64{dgeo, dkappa, dmb, dps, dpgeo, dslaboff, dslab, ddirs, dscr, n64,
+                               counters + 3, dorder + n32, 0, gcd_min_tree};
+                if (n32) { k_setup<32, 0><<<grid32, 32, smem32>>>(SA32); ++launches; }
+                if (n64) { k_setup<MH, 0><<<grid64, 128>>>(SA64); ++launches; }
+                SA32.next = counters + 1; SA64.next = counters + 4;
+                if (n32) { k_setup<32, 1><<<grid32, 32, smem32>>>(SA32); ++launches; }
+                if (n64) { k_setup<MH, 1><<<grid64, 128>>>(SA64); ++launches; }
+                SA32.next = counters + 2; SA64.next = counters + 5;
+                if (n32) { k_setup<32, 2><<<grid32, 32, smem32>>>(SA32); ++launches; }
+                if (n64) { k_setup<MH, 2><<<grid64, 128>>>(SA64); ++launches; }
+                CK(cudaGetLastError());
             }
             CK(cudaEventRecord(ev[1]));
             // ---- search ----

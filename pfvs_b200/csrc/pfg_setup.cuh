@@ -589,9 +589,16 @@ PFG_NOINLINE __device__ int warp_unimodular(const int64_t *vin, int n, int64_t *
 #endif
 
 // ---------------------------------------------------------------------------
-// The setup of one direction; S is the warp's LLL working set (N >= h11).
+// The setup of one direction in three phases, each a kernel of its own in the
+// batched path so that the warps of an SM run the same code (the phases'
+// code together does not fit the instruction caches).  They share only the
+// direction's slab (BT, ZT, MAT, U, H) and Dir; S is the warp's LLL working
+// set (N >= h11).  Each returns ST_PENDING to go on, else the final status.
+//   phase 0: steps 1-7 (Z, v, orthogonal lattice, Euclidean LLL, Binter, mat)
+//   phase 1: step 8 (cut-aware basis)
+//   phase 2: steps 10, 9, 11 (Cholesky and certificate, GCD rows, bounds)
 // ---------------------------------------------------------------------------
-template <int N> __device__ int setup_one(const SetupArgs &A, int pid, int lane, int &stage, LllMem<N> *S)
+template <int N> __device__ int setup_phase0(const SetupArgs &A, int pid, int lane, int &stage, LllMem<N> *S)
 {
     SetupScratch *W = A.scratch + (blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5));
     const Geo g = A.geo[A.pgeo[pid]];
@@ -602,6 +609,7 @@ template <int N> __device__ int setup_one(const SetupArgs &A, int pid, int lane,
     Dir &D = A.dirs[pid];
     bool bad = false;
     StageClock clk(stage, lane);
+    (void)D;
 
     clk.mark(1);
     // 1. Z = kappa . p
@@ -690,7 +698,23 @@ template <int N> __device__ int setup_one(const SetupArgs &A, int pid, int lane,
     }
     __syncwarp();
     if (warp_any(bad)) return ST_OVERFLOW;
+    return ST_PENDING;
+}
 
+template <int N> __device__ int setup_phase1(const SetupArgs &A, int pid, int lane, int &stage, LllMem<N> *S)
+{
+    SetupScratch *W = A.scratch + (blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5));
+    const Geo g = A.geo[A.pgeo[pid]];
+    const int h = g.h, d = h - 1;
+    const int64_t *kap = A.kappa + g.koff, *Mb = A.Mbasis + g.moff, *p = A.ps + (int64_t)pid * MH;
+    int64_t *slab = A.slab + A.slab_off[pid];
+    const Slab L = slab_layout(h, d);
+    Dir &D = A.dirs[pid];
+    bool bad = false;
+    StageClock clk(stage, lane);
+    (void)kap; (void)Mb; (void)p;
+    int64_t *BT = slab + L.bt, *ZT = slab + L.zt, *MAT = slab + L.mat;
+    int st = 0;
     clk.mark(8);
     // 8. cut-aware basis (pfv_lattice.h:554-602)
     for (int a = lane; a < d; a += 32) W->v[a] = BT[a * h];
@@ -765,7 +789,26 @@ template <int N> __device__ int setup_one(const SetupArgs &A, int pid, int lane,
         if (lane == 0) { D.m0_level = -1; D.g_lin = 0; }
         return ST_EMPTY;
     }
+    if (lane == 0) { D.m0_level = m0_level; D.g_lin = g_lin; }
+    __syncwarp();
+    return ST_PENDING;
+}
 
+template <int N> __device__ int setup_phase2(const SetupArgs &A, int pid, int lane, int &stage, LllMem<N> *S)
+{
+    SetupScratch *W = A.scratch + (blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5));
+    const Geo g = A.geo[A.pgeo[pid]];
+    const int h = g.h, d = h - 1;
+    const int64_t *kap = A.kappa + g.koff, *Mb = A.Mbasis + g.moff, *p = A.ps + (int64_t)pid * MH;
+    int64_t *slab = A.slab + A.slab_off[pid];
+    const Slab L = slab_layout(h, d);
+    Dir &D = A.dirs[pid];
+    bool bad = false;
+    StageClock clk(stage, lane);
+    (void)kap; (void)Mb;
+    int64_t *BT = slab + L.bt, *ZT = slab + L.zt, *MAT = slab + L.mat;
+    const int m0_level = D.m0_level;
+    const int64_t g_lin = D.g_lin;
     clk.mark(10);
     // 10. FP64 Cholesky of mat, certificate, float copies
     double *U = (double *)(slab + L.u64);
@@ -961,8 +1004,6 @@ h_done:
     }
     if (warp_any(bad)) return ST_OVERFLOW;
     if (lane == 0) {
-        D.m0_level = m0_level;
-        D.g_lin = g_lin;
         D.hrows = hrows;
         D.slack_chol = slack_chol;
     }
@@ -970,11 +1011,29 @@ h_done:
     return ST_PENDING;
 }
 
-// Persistent setup kernel: warps take directions from A.todo through an
-// atomic counter.  N = 32 serves h11 <= 32 with the LLL working set in
+template <int N, int PH> __device__ __forceinline__ int setup_phase(const SetupArgs &A, int pid, int lane, int &stage,
+                                                                   LllMem<N> *S)
+{
+    if (PH == 0) return setup_phase0<N>(A, pid, lane, stage, S);
+    if (PH == 1) return setup_phase1<N>(A, pid, lane, stage, S);
+    return setup_phase2<N>(A, pid, lane, stage, S);
+}
+
+// All three phases of one direction in sequence (the no-allocation entry point).
+template <int N> __device__ int setup_one(const SetupArgs &A, int pid, int lane, int &stage, LllMem<N> *S)
+{
+    int st = setup_phase0<N>(A, pid, lane, stage, S);
+    if (st == ST_PENDING) st = setup_phase1<N>(A, pid, lane, stage, S);
+    if (st == ST_PENDING) st = setup_phase2<N>(A, pid, lane, stage, S);
+    return st;
+}
+
+// Persistent setup kernel of phase PH: warps take directions from A.todo
+// through an atomic counter; phases 1 and 2 skip the directions an earlier
+// phase finished.  N = 32 serves h11 <= 32 with the LLL working set in
 // dynamic shared memory (one LllMem<32> per warp) when A.smem_core is set;
 // otherwise (and for N = 64) the working set is the warp's global scratch.
-template <int N> __global__ void __launch_bounds__(128) k_setup(SetupArgs A)
+template <int N, int PH> __global__ void __launch_bounds__(128) k_setup(SetupArgs A)
 {
 #ifdef PFG_EMU
     unsigned char *smem_raw = nullptr;
@@ -991,14 +1050,18 @@ template <int N> __global__ void __launch_bounds__(128) k_setup(SetupArgs A)
         if (t >= (unsigned)A.n) break;
         const int pid = A.todo ? A.todo[t] : (int)t;
         const Geo g = A.geo[A.pgeo[pid]];
-        if (lane == 0) {
-            Dir &D = A.dirs[pid];
-            D.geo = A.pgeo[pid]; D.h = g.h; D.d = g.h - 1; D.slab = A.slab_off[pid];
-            D.m0_level = -1; D.g_lin = 0; D.hrows = 0; D.slack_chol = 0.0;
+        if (PH == 0) {
+            if (lane == 0) {
+                Dir &D = A.dirs[pid];
+                D.geo = A.pgeo[pid]; D.h = g.h; D.d = g.h - 1; D.slab = A.slab_off[pid];
+                D.m0_level = -1; D.g_lin = 0; D.hrows = 0; D.slack_chol = 0.0;
+            }
+        } else if (A.dirs[pid].status != ST_PENDING) {
+            continue;
         }
         __syncwarp();
         int stage = 0;
-        int st = g.h <= N ? setup_one<N>(A, pid, lane, stage, S) : ST_OVERFLOW;
+        int st = g.h <= N ? setup_phase<N, PH>(A, pid, lane, stage, S) : ST_OVERFLOW;
         if (lane == 0) { A.dirs[pid].status = st; A.dirs[pid].pad = st < 0 ? stage : 0; }
         __syncwarp();
     }

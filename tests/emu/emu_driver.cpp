@@ -70,8 +70,15 @@ extern "C" int emu_coni_batch(const pfg_input *in, int precision, int n_warps, p
     SetupArgs SA64 = SA;
     SA64.n = (int)o64.size(); SA64.next = &next64; SA64.todo = o64.data();
     fprintf(stderr, "emu: setup\n");
-    if (!o32.empty()) launch(setup_warps, [&] { k_setup<32>(SA); });
-    if (!o64.empty()) launch(setup_warps, [&] { k_setup<MH>(SA64); });
+    // the three phase kernels in order, each with a fresh work counter
+    if (!o32.empty()) launch(setup_warps, [&] { k_setup<32, 0>(SA); });
+    if (!o64.empty()) launch(setup_warps, [&] { k_setup<MH, 0>(SA64); });
+    next = 0; next64 = 0;
+    if (!o32.empty()) launch(setup_warps, [&] { k_setup<32, 1>(SA); });
+    if (!o64.empty()) launch(setup_warps, [&] { k_setup<MH, 1>(SA64); });
+    next = 0; next64 = 0;
+    if (!o32.empty()) launch(setup_warps, [&] { k_setup<32, 2>(SA); });
+    if (!o64.empty()) launch(setup_warps, [&] { k_setup<MH, 2>(SA64); });
     fprintf(stderr, "emu: setup done\n");
 
     const unsigned long long pts_cap = 1 << 20;
