@@ -87,7 +87,7 @@ typedef struct {
     int form;                  /* PFG_FORM_* */
     int precision;             /* PFG_PREC_* */
     int blocks_per_sm;         /* persistent search grid (0: default) */
-    int warps_per_block;       /* (0: default) */
+    int warps_per_block;       /* (0: default, 4; at most 4) */
     double gcd_min_tree;       /* GCD-cut rows are built for a direction whose estimated
                                   search tree has at least this many nodes (they only
                                   prune; results are identical either way).  0: the

@@ -505,7 +505,7 @@ static int coni_run(const pfg_input *in, const pfg_options *opt_in, pfg_output *
                 const unsigned st32 = stage_bytes<float>(hmax - 1, hmax), st64 = stage_bytes<double>(hmax - 1, hmax);
                 const int smem_max = 227 * 1024;
                 auto warps_for = [&](unsigned st) {
-                    const int w = opt.warps_per_block > 0 ? opt.warps_per_block : 8;
+                    const int w = opt.warps_per_block > 0 ? std::min(opt.warps_per_block, SEARCH_WARPS) : SEARCH_WARPS;
                     return std::max(1, std::min(w, smem_max / (int)st));
                 };
                 const int wpb32 = warps_for(st32), wpb64 = warps_for(st64);

@@ -201,6 +201,19 @@ template <class R> __device__ __forceinline__ bool gcd_fails(u128 g, int64_t Q, 
 
 struct Tally { unsigned long long nodes, cands, leaves; };
 
+// Profiling build only (-DPFG_STAGE_CLOCKS): per pass (float 0, double 1)
+// the warps' clock64() cycles spent searching [0/1] and waiting for work
+// [2/3], the subtrees run [4/5], and within the search the cycles of the
+// leaf level (exact q, GCD cut, emission) [6/7].
+#ifdef PFG_STAGE_CLOCKS
+__device__ unsigned long long pfg_search_cycles[8];
+#define PFG_SCLK(v) long long v = clock64()
+#define PFG_SADD(i, x) do { if (lane == 0) atomicAdd(&pfg_search_cycles[(i) + (sizeof(R) == 8)], (unsigned long long)(x)); } while (0)
+#else
+#define PFG_SCLK(v) do { } while (0)
+#define PFG_SADD(i, x) do { } while (0)
+#endif
+
 // Per-lane register state: levels lane (slot 0) and lane + 32 (slot 1).
 template <class R> struct Lanes {
     int64_t cur0, cur1, hi0, hi1;
@@ -481,6 +494,7 @@ __device__ int run_subtree(const SearchArgs &A, const Prob<R> &P, int pid, const
         // leaves: exact q, exact gcd of Kn[1:], emission
         LSET(S, cur, i, cur + ncand);
         if (!mask) continue;
+        PFG_SCLK(c_leaf);
         T.leaves += __popc(mask);
         bool ok = pass;
         i128 q = 0;
@@ -501,7 +515,11 @@ __device__ int run_subtree(const SearchArgs &A, const Prob<R> &P, int pid, const
             if (g != 0 && (i128)P.Q * (i128)g <= qt && lane == t) ok = false;
         }
         unsigned emit = __ballot_sync(FULL, ok);
+#ifdef PFG_STAGE_CLOCKS
+        if (!emit) { PFG_SCLK(c_leaf_end); PFG_SADD(6, c_leaf_end - c_leaf); continue; }
+#else
         if (!emit) continue;
+#endif
         unsigned long long base = 0;
         if (lane == 0) base = atomicAdd(A.npts, (unsigned long long)__popc(emit));
         base = __shfl_sync(FULL, base, 0);
@@ -523,6 +541,10 @@ __device__ int run_subtree(const SearchArgs &A, const Prob<R> &P, int pid, const
             else if (lane < d) cc[lane] = S.c0;
             if (lane + 32 < d) cc[lane + 32] = S.c1;
         }
+#ifdef PFG_STAGE_CLOCKS
+        PFG_SCLK(c_leaf_end);
+        PFG_SADD(6, c_leaf_end - c_leaf);
+#endif
     }
     return 0;
 }
@@ -549,20 +571,11 @@ static unsigned char emu_stage[64 * 1024];
 #define PFG_STAGE_AREA(A) ((void *)(pfg_stage_smem + (threadIdx.x >> 5) * (A).stage_bytes))
 #endif
 
-// Profiling build only (-DPFG_STAGE_CLOCKS): per pass (float 0, double 1)
-// the warps' clock64() cycles spent searching [0/1] and waiting for work
-// [2/3], and the subtrees run [4/5].
-#ifdef PFG_STAGE_CLOCKS
-__device__ unsigned long long pfg_search_cycles[8];
-#define PFG_SCLK(v) long long v = clock64()
-#define PFG_SADD(i, x) do { if (lane == 0) atomicAdd(&pfg_search_cycles[(i) + (sizeof(R) == 8)], (unsigned long long)(x)); } while (0)
-#else
-#define PFG_SCLK(v) do { } while (0)
-#define PFG_SADD(i, x) do { } while (0)
-#endif
-
+// Blocks of at most SEARCH_WARPS warps, three per SM: the search's registers
+// (about 165 per thread) then fit without spilling to local memory.
+constexpr int SEARCH_WARPS = 4;
 template <class R>
-__global__ void __launch_bounds__(256, 2) k_search(SearchArgs A)
+__global__ void __launch_bounds__(SEARCH_WARPS * 32, 3) k_search(SearchArgs A)
 {
 #ifndef PFG_EMU
     extern __shared__ __align__(16) unsigned char pfg_stage_smem[];
