@@ -39,14 +39,19 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-# Roofline of the dominant kernel (k_setup<32>, the per-direction lattice
-# setup): scalar integer / FP64 warp code, neither HBM- nor tensor-bound, so
-# its ceiling is the warp-instruction issue rate, 148 SMs x 4 schedulers x
-# SM clock.  Per-unit figures from one ncu capture of the kernel on the
-# first 16,384 directions of this batch (profiles/k_setup_mixed.md):
-# executed warp instructions and DRAM bytes per direction.
-SETUP_INST_PER_DIR = 17_400_906_604 / 16384
-SETUP_DRAM_PER_DIR = (95_471_616 + 593_945_856) / 16384
+# Roofline of the dominant kernel, k_search<double> (the persistent
+# FP64-pruned search, about 38 % of the launch list): scalar integer / FP64
+# warp code, neither HBM- nor tensor-bound, so its ceiling is the
+# warp-instruction issue rate, 148 SMs x 4 schedulers x SM clock.  Per-unit
+# figures from one ncu --set full capture of the timed form's search on the
+# first 16,384 directions of this batch (20,582,107 nodes): executed warp
+# instructions and DRAM bytes per search node.
+SEARCH_INST_PER_NODE = 17_437_909_937 / 20_582_107
+SEARCH_DRAM_PER_NODE = (244_797_696 + 107_985_664) / 20_582_107
+# The setup's three phase kernels (k_setup<32, 0..2>) together, from the
+# same kind of capture on the same 16,384 directions: per direction.
+SETUP_INST_PER_DIR = (3_785_943_035 + 6_529_456_061 + 1_841_800_499) / 16384
+SETUP_DRAM_PER_DIR = (10_734_080 + 253_480_192 + 191_088_384 + 196_837_376 + 215_589_376 + 138_622_720) / 16384
 N_SM, SCHEDULERS = 148, 4
 
 
@@ -341,20 +346,29 @@ def main():
                "device_ms": allmax(pg, secs_p) * 1e3,
                "pfvs_per_s": allsum(pg, len(pp)) / max(allmax(pg, secs_p), 1e-12)}
         del Kp, Mp, pp
-    # roofline of the setup kernel: executed warp instructions per launch (ncu
-    # per-direction figure x directions) over its CUDA-event time
+    # roofline of the search kernel: executed warp instructions per launch (ncu
+    # per-node figure x the launch's nodes) over its CUDA-event time (the
+    # search stage: k_flip, a few microseconds, then k_search<double>); the
+    # setup's three phase kernels beside it, per direction
     peaks, peaks_kind = measured_peaks()
     clk_sum = clk.summary()
     mhz = clk_sum.get("sm_mhz") or peaks.get("sm_max_mhz", 1965.0)
-    setup_s = stats["ms_setup"] / 1e3
-    achieved = SETUP_INST_PER_DIR * len(idx) / setup_s
     peak = N_SM * SCHEDULERS * mhz * 1e6
-    roofline = {"kernel": "k_setup<32>", "bound": "issue", "achieved": achieved, "peak": peak,
+    search_s = stats["ms_search"] / 1e3
+    achieved = SEARCH_INST_PER_NODE * stats["nodes"] / search_s
+    roofline = {"kernel": "k_search<double>", "bound": "issue", "achieved": achieved, "peak": peak,
                 "unit": "warp-inst/s", "frac": achieved / peak,
-                "traffic": SETUP_DRAM_PER_DIR * len(idx),
-                "basis": f"ncu: {SETUP_INST_PER_DIR:.0f} warp-inst and {SETUP_DRAM_PER_DIR:.0f} DRAM bytes per "
-                         f"direction; peak = {N_SM} SMs x {SCHEDULERS} x {mhz:.0f} MHz (sampled SM clock); "
-                         f"HBM for context: {peaks.get('hbm_gbs')} GB/s {peaks_kind}"}
+                "traffic": SEARCH_DRAM_PER_NODE * stats["nodes"],
+                "basis": f"ncu: {SEARCH_INST_PER_NODE:.0f} warp-inst and {SEARCH_DRAM_PER_NODE:.1f} DRAM bytes per "
+                         f"search node x {stats['nodes']} nodes per launch; peak = {N_SM} SMs x {SCHEDULERS} x "
+                         f"{mhz:.0f} MHz (sampled SM clock); HBM for context: {peaks.get('hbm_gbs')} GB/s {peaks_kind}"}
+    setup_s = stats["ms_setup"] / 1e3
+    setup_ach = SETUP_INST_PER_DIR * len(idx) / setup_s
+    roofline_setup = {"kernel": "k_setup<32, 0..2>", "bound": "issue", "achieved": setup_ach, "peak": peak,
+                      "unit": "warp-inst/s", "frac": setup_ach / peak,
+                      "traffic": SETUP_DRAM_PER_DIR * len(idx),
+                      "basis": f"ncu: {SETUP_INST_PER_DIR:.0f} warp-inst and {SETUP_DRAM_PER_DIR:.0f} DRAM bytes "
+                               f"per direction over the three phases x {len(idx)} directions"}
     if rank == 0:
         line = {"metric": "lattice nodes/s", "value": value, "unit": "nodes/s", "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup,
@@ -373,7 +387,7 @@ def main():
                 "stage_ms": {"setup": stats["ms_setup"], "search": stats["ms_search"],
                              "output": stats["ms_output"]},
                 "fp32_nodes_per_step": stats["nodes"], "wall_ms_per_step": wall_s / args.steps * 1e3,
-                "clocks": clk_sum, "e2e": e2e, "cpu_baseline": cpu, "roofline": roofline, "pfvs": pfv,
+                "clocks": clk_sum, "e2e": e2e, "cpu_baseline": cpu, "roofline": roofline, "roofline_setup": roofline_setup, "pfvs": pfv,
                 "gpu_launches": int(stats.get("launches", 0)) * args.steps}
         print(json.dumps(line))
     if pg is not None:
