@@ -311,12 +311,12 @@ template <class R> __device__ __forceinline__ int level_range(const Prob<R> &P, 
 }
 
 // Enter level i (warp search): the level's sums and candidate range into
-// the lanes' registers.  Returns ST_RANGE if a bound leaves int32.
+// the owner lanes' registers (kept for the return to this level and for
+// donation), and to the caller (every lane).  Returns ST_RANGE if a bound
+// leaves int32.
 template <class R> __device__ int enter_level(Lanes<R> &S, const Prob<R> &P, int i, R rem, R err, u128 gab,
-                                              int lane, int64_t &lo_o, int64_t &hi_o)
+                                              int lane, int64_t &lo_o, int64_t &hi_o, R &off, R &aoff, i128 &pre)
 {
-    R off, aoff;
-    i128 pre;
     level_sums(S, P, i, lane, off, aoff, pre);
     int64_t lo, hi;
     const int st = level_range(P, i, rem, err, gab, off, aoff, lo, hi);
@@ -350,10 +350,16 @@ __device__ int run_subtree(const SearchArgs &A, const Prob<R> &P, int pid, const
     S.gab0 = S.gab1 = 0; S.pre0 = S.pre1 = 0;
     S.c0 = S.c1 = 0; S.y0 = S.y1 = S.k0 = S.k1 = 0;
     int top, i;
+    // The current level's entry values, the same in every lane (its owner
+    // lane keeps a copy for the return to it after the levels below).
+    int64_t u_cur, u_hi;
+    R u_rem, u_err, u_off, u_aoff;
+    u128 u_gab;
+    i128 u_pre;
     if (!it) {                                    // the root of the direction
         top = i = d - 1;
-        int64_t lo, hi;
-        int st = enter_level(S, P, i, P.qmax_r, P.Kerr * P.qmax_r, (u128)0, lane, lo, hi);
+        u_rem = P.qmax_r; u_err = P.Kerr * P.qmax_r; u_gab = 0;
+        int st = enter_level(S, P, i, u_rem, u_err, u_gab, lane, u_cur, u_hi, u_off, u_aoff, u_pre);
         if (st) return st;
         T.nodes++;
     } else {                                      // a donated node
@@ -373,6 +379,8 @@ __device__ int run_subtree(const SearchArgs &A, const Prob<R> &P, int pid, const
         LSET(S, rem, i, (R)it->rem); LSET(S, err, i, (R)it->err);
         LSET(S, off, i, off); LSET(S, aoff, i, aoff);
         LSET(S, gab, i, gab); LSET(S, pre, i, pre);
+        u_cur = it->cur; u_hi = it->hi; u_rem = (R)it->rem; u_err = (R)it->err;
+        u_off = off; u_aoff = aoff; u_gab = gab; u_pre = pre;
     }
     const R slack = P.slack, Kerr = P.Kerr;
     // leaf data for the current level-0 node: q(v) = A0 + 2 v B0 + m00 v^2
@@ -384,13 +392,20 @@ __device__ int run_subtree(const SearchArgs &A, const Prob<R> &P, int pid, const
     const unsigned long long t0 = shfl(gtimer(), 0);
     for (;;) {
         if (i > top) break;
-        int64_t cur = LGET(S, cur, i), hi = LGET(S, hi, i);
-        if (cur > hi) {                           // backtrack
+        if (u_cur > u_hi) {                       // backtrack
             int32_t ci = LGET(S, c, i);
             if (ci) { apply_dc(S, P, i, -(int64_t)ci, lane); LSET(S, c, i, 0); }
             ++i;
+            if (i <= top) {                       // the parent's values from its owner lane
+                u_cur = LGET(S, cur, i); u_hi = LGET(S, hi, i);
+                u_rem = LGET(S, rem, i); u_err = LGET(S, err, i);
+                u_off = LGET(S, off, i); u_aoff = LGET(S, aoff, i);
+                u_gab = shflu128(i < 32 ? S.gab0 : S.gab1, i & 31);
+                u_pre = shfl128(i < 32 ? S.pre0 : S.pre1, i & 31);
+            }
             continue;
         }
+        const int64_t cur = u_cur, hi = u_hi;
         // donate the top of the stack when other warps are idle
         if (((++poll) & 4095) == 0 && (long long)(shfl(gtimer(), 0) - t0) > A.deadline_ns)
             return ST_WAIT;                       // (uniform: lane 0's clock)
@@ -427,14 +442,14 @@ __device__ int run_subtree(const SearchArgs &A, const Prob<R> &P, int pid, const
                         __threadfence();
                         __syncwarp();
                         if (lane == 0) { atomicExch(&A.ready[slot], 1); atomicAdd(&A.ctl->donated, 1ull); }
-                        LSET(S, hi, j, jc - 1);
+                        LSET(S, hi, j, jc - 1);       // (j > i: not the current level)
                     }
                 }
             }
         }
-        const R rem = LGET(S, rem, i), err = LGET(S, err, i), off = LGET(S, off, i), aoff = LGET(S, aoff, i);
-        const u128 gab = shflu128(i < 32 ? S.gab0 : S.gab1, i & 31);
-        const i128 pre = shfl128(i < 32 ? S.pre0 : S.pre1, i & 31);
+        const R rem = u_rem, err = u_err, off = u_off, aoff = u_aoff;
+        const u128 gab = u_gab;
+        const i128 pre = u_pre;
         const bool hrow = (P.hrows >> i) & 1;
         const int64_t hii = hrow ? P.H[i * d + i] : 0;
         const R uii = P.U[upk(i, i, d)];
@@ -474,25 +489,26 @@ __device__ int run_subtree(const SearchArgs &A, const Prob<R> &P, int pid, const
         T.cands += (unsigned long long)ncand;
         unsigned mask = __ballot_sync(FULL, pass);
         if (i > 0) {
-            if (!mask) { LSET(S, cur, i, cur + ncand); continue; }
+            if (!mask) { u_cur = cur + ncand; continue; }
             const int t0 = __ffs(mask) - 1;
             const int64_t vc = cur + t0;
-            LSET(S, cur, i, vc + 1);
+            u_cur = vc + 1;
+            LSET(S, cur, i, u_cur);               // (for the return to this level and for donation)
             const R nr0 = shfl(nr, t0), en0 = shfl(en, t0);
             const u128 g0 = shflu128(gn, t0);
             const int32_t ci = LGET(S, c, i);
             apply_dc(S, P, i, vc - ci, lane);
             LSET(S, c, i, (int32_t)vc);
             --i;
-            int64_t lo, hh;
-            int st = enter_level(S, P, i, nr0, en0, g0, lane, lo, hh);
+            u_rem = nr0; u_err = en0; u_gab = g0;
+            int st = enter_level(S, P, i, u_rem, u_err, u_gab, lane, u_cur, u_hi, u_off, u_aoff, u_pre);
             if (st) return st;
             T.nodes++;
             if (i == 0) leaf_data(S, P, lane, A0, B0);
             continue;
         }
         // leaves: exact q, exact gcd of Kn[1:], emission
-        LSET(S, cur, i, cur + ncand);
+        u_cur = cur + ncand;
         if (!mask) continue;
         PFG_SCLK(c_leaf);
         T.leaves += __popc(mask);
