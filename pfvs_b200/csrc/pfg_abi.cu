@@ -276,8 +276,8 @@ extern "C" int pfg_debug_stage_cycles(unsigned long long *out)
 // profiling build only: the search's busy / waiting cycles and subtree counts (and zero them)
 extern "C" int pfg_debug_search_cycles(unsigned long long *out)
 {
-    if (cudaMemcpyFromSymbol(out, pfg::pfg_search_cycles, sizeof(unsigned long long) * 8) != cudaSuccess) return 1;
-    unsigned long long z[8] = {};
+    if (cudaMemcpyFromSymbol(out, pfg::pfg_search_cycles, sizeof(unsigned long long) * 16) != cudaSuccess) return 1;
+    unsigned long long z[16] = {};
     return cudaMemcpyToSymbol(pfg::pfg_search_cycles, z, sizeof z) != cudaSuccess;
 }
 #endif

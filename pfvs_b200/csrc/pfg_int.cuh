@@ -114,6 +114,41 @@ PFG_HD uint64_t gcd64_ge(uint64_t u, uint64_t v, uint64_t need)
     return u << sh;
 }
 
+PFG_HD int ctz32(uint32_t x)
+{
+#ifdef __CUDA_ARCH__
+    return __ffs((int)x) - 1;
+#else
+    return __builtin_ctz(x);
+#endif
+}
+
+// gcd64_ge on 32-bit operands (u != 0)
+PFG_HD uint64_t gcd32_ge(uint32_t u, uint32_t v, uint64_t need)
+{
+    if (v == 0) return u >= need ? u : 0;
+    const int sh = ctz32(u | v);
+    const uint64_t need_s = (need >> sh) + ((need & ((1ULL << sh) - 1)) != 0);
+    u >>= ctz32(u);
+    do {
+        v >>= ctz32(v);
+        if (u > v) { uint32_t t = v; v = u; u = t; }
+        if (u < need_s) return 0;
+        v -= u;
+    } while (v);
+    return (uint64_t)u << sh;
+}
+
+// gcd64_ge(u, v, need) for a small u and a large v, the usual case of the
+// search's GCD-row test (u = the gcd of the rows above): the binary
+// algorithm needs about one step per bit of v there, so v is first reduced
+// modulo u (gcd(u, v) = gcd(u, v mod u)) and the rest runs in 32 bits.
+PFG_HD uint64_t gcd64_ge_small(uint64_t u, uint64_t v, uint64_t need)
+{
+    if (u != 0 && (u >> 32) == 0 && v > u) return gcd32_ge((uint32_t)u, (uint32_t)(v % u), need);
+    return gcd64_ge(u, v, need);
+}
+
 PFG_HD u128 gcd128(u128 u, u128 v)
 {
     if ((u >> 64) == 0 && (v >> 64) == 0) return gcd64((uint64_t)u, (uint64_t)v);

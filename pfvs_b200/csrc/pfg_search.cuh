@@ -204,9 +204,11 @@ struct Tally { unsigned long long nodes, cands, leaves; };
 // Profiling build only (-DPFG_STAGE_CLOCKS): per pass (float 0, double 1)
 // the warps' clock64() cycles spent searching [0/1] and waiting for work
 // [2/3], the subtrees run [4/5], and within the search the cycles of the
-// leaf level (exact q, GCD cut, emission) [6/7].
+// leaf level (exact q, GCD cut, emission) [6/7]; in the FP64 pass the
+// cycles of backtracks [8], candidate evaluation at interior levels [9] and
+// descents (incremental sums, entering the level) [10].
 #ifdef PFG_STAGE_CLOCKS
-__device__ unsigned long long pfg_search_cycles[8];
+__device__ unsigned long long pfg_search_cycles[16];
 #define PFG_SCLK(v) long long v = clock64()
 #define PFG_SADD(i, x) do { if (lane == 0) atomicAdd(&pfg_search_cycles[(i) + (sizeof(R) == 8)], (unsigned long long)(x)); } while (0)
 #else
@@ -390,8 +392,14 @@ __device__ int run_subtree(const SearchArgs &A, const Prob<R> &P, int pid, const
     const int64_t m00 = (int64_t)P.MAT[0];
     unsigned poll = 0;
     const unsigned long long t0 = shfl(gtimer(), 0);
+#ifdef PFG_STAGE_CLOCKS
+    long long acc_bt = 0, acc_ev = 0, acc_ds = 0, acc_gcd = 0;
+#endif
     for (;;) {
         if (i > top) break;
+#ifdef PFG_STAGE_CLOCKS
+        const long long k0 = clock64();
+#endif
         if (u_cur > u_hi) {                       // backtrack
             int32_t ci = LGET(S, c, i);
             if (ci) { apply_dc(S, P, i, -(int64_t)ci, lane); LSET(S, c, i, 0); }
@@ -403,6 +411,9 @@ __device__ int run_subtree(const SearchArgs &A, const Prob<R> &P, int pid, const
                 u_gab = shflu128(i < 32 ? S.gab0 : S.gab1, i & 31);
                 u_pre = shfl128(i < 32 ? S.pre0 : S.pre1, i & 31);
             }
+#ifdef PFG_STAGE_CLOCKS
+            acc_bt += clock64() - k0;
+#endif
             continue;
         }
         const int64_t cur = u_cur, hi = u_hi;
@@ -468,6 +479,9 @@ __device__ int run_subtree(const SearchArgs &A, const Prob<R> &P, int pid, const
             else if (nr < -(slack + en)) pass = false;
         }
         if (pass && i == P.m0_level && (i128)P.g_lin * v < (i128)P.linmin) pass = false;
+#ifdef PFG_STAGE_CLOCKS
+        const long long kg0 = clock64();
+#endif
         if (pass) {
             const R q_lb = (P.qmax_r - nr) - (slack + en);
             if (hrow) {
@@ -475,7 +489,7 @@ __device__ int run_subtree(const SearchArgs &A, const Prob<R> &P, int pid, const
                 else {
                     u128 a = uabs(pre + (i128)hii * v);
                     if ((gn >> 64) == 0 && (a >> 64) == 0 && (gn | a) != 0) {
-                        uint64_t gg = gcd64_ge((uint64_t)gn, (uint64_t)a, need_of(q_lb, P.Q));
+                        uint64_t gg = gcd64_ge_small((uint64_t)gn, (uint64_t)a, need_of(q_lb, P.Q));
                         if (!gg) pass = false;
                         gn = gg;
                     } else {
@@ -485,9 +499,17 @@ __device__ int run_subtree(const SearchArgs &A, const Prob<R> &P, int pid, const
             }
             if (pass && gcd_fails(gn, P.Q, q_lb)) pass = false;
         }
+#ifdef PFG_STAGE_CLOCKS
+        __syncwarp();
+        acc_gcd += clock64() - kg0;
+#endif
         if (__any_sync(FULL, ferr)) return ST_FLOAT;
         T.cands += (unsigned long long)ncand;
         unsigned mask = __ballot_sync(FULL, pass);
+#ifdef PFG_STAGE_CLOCKS
+        const long long k1 = clock64();
+        acc_ev += k1 - k0;
+#endif
         if (i > 0) {
             if (!mask) { u_cur = cur + ncand; continue; }
             const int t0 = __ffs(mask) - 1;
@@ -505,6 +527,9 @@ __device__ int run_subtree(const SearchArgs &A, const Prob<R> &P, int pid, const
             if (st) return st;
             T.nodes++;
             if (i == 0) leaf_data(S, P, lane, A0, B0);
+#ifdef PFG_STAGE_CLOCKS
+            acc_ds += clock64() - k1;
+#endif
             continue;
         }
         // leaves: exact q, exact gcd of Kn[1:], emission
@@ -562,6 +587,14 @@ __device__ int run_subtree(const SearchArgs &A, const Prob<R> &P, int pid, const
         PFG_SADD(6, c_leaf_end - c_leaf);
 #endif
     }
+#ifdef PFG_STAGE_CLOCKS
+    if (lane == 0 && sizeof(R) == 8) {
+        atomicAdd(&pfg_search_cycles[8], (unsigned long long)acc_bt);
+        atomicAdd(&pfg_search_cycles[9], (unsigned long long)acc_ev);
+        atomicAdd(&pfg_search_cycles[10], (unsigned long long)acc_ds);
+        atomicAdd(&pfg_search_cycles[11], (unsigned long long)acc_gcd);
+    }
+#endif
     return 0;
 }
 
