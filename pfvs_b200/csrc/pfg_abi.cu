@@ -509,15 +509,20 @@ static int coni_run(const pfg_input *in, const pfg_options *opt_in, pfg_output *
                     return std::max(1, std::min(w, smem_max / (int)st));
                 };
                 const int wpb32 = warps_for(st32), wpb64 = warps_for(st64);
-                CK(cudaFuncSetAttribute(k_search<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, wpb32 * st32));
-                CK(cudaFuncSetAttribute(k_search<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, wpb64 * st64));
+                // one level per lane (NS = 1) when every h11 of the batch is <= 32, else two
+                const bool one = hmax <= 32;
+                void (*ks32)(SearchArgs) = one ? k_search<float, 1> : k_search<float, 2>;
+                void (*ks64)(SearchArgs) = one ? k_search<double, 1> : k_search<double, 2>;
+                void (*kplain)(SearchArgs, int) = one ? k_search_plain<double, 1> : k_search_plain<double, 2>;
+                CK(cudaFuncSetAttribute((const void *)ks32, cudaFuncAttributeMaxDynamicSharedMemorySize, wpb32 * st32));
+                CK(cudaFuncSetAttribute((const void *)ks64, cudaFuncAttributeMaxDynamicSharedMemorySize, wpb64 * st64));
                 if (opt.form == PFG_FORM_PLAIN) {
                     // one launch, one warp per direction, FP64 pruning, no work sharing
-                    CK(cudaFuncSetAttribute(k_search_plain<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, st64));
+                    CK(cudaFuncSetAttribute((const void *)kplain, cudaFuncAttributeMaxDynamicSharedMemorySize, st64));
                     k_flip<<<(nb + 255) / 256, 256>>>(ddirs, dgeo, nb, 0, ddirpass, dretry); ++launches;
                     A.donate = 0; A.n_warps = 1; A.ctl = dctl + 1; A.pass = 2; A.stage_bytes = st64;
                     A.todo = dtodoall; A.n_todo = nb;
-                    k_search_plain<double><<<nb, 32, st64>>>(A, -1); ++launches;
+                    kplain<<<nb, 32, st64>>>(A, -1); ++launches;
                     CK(cudaGetLastError());
                 } else {
                     auto grid_for = [&](const void *fn, int wpb, unsigned st, int &grid) -> cudaError_t {
@@ -535,21 +540,21 @@ static int coni_run(const pfg_input *in, const pfg_options *opt_in, pfg_output *
                     // FP32 pass over the FP32 geometries' directions
                     if (!todo32.empty()) {
                         int grid = 0;
-                        CK(grid_for((const void *)k_search<float>, wpb32, st32, grid));
+                        CK(grid_for((const void *)ks32, wpb32, st32, grid));
                         A.n_warps = grid * wpb32; A.stage_bytes = st32;
                         A.ctl = dctl; A.todo = dtodo32; A.n_todo = (int)todo32.size(); A.pass = 1;
                         CK(cudaMemset(dready, 0, (size_t)q_cap * 4));
-                        k_search<float><<<grid, wpb32 * 32, (size_t)wpb32 * st32>>>(A); ++launches;
+                        ks32<<<grid, wpb32 * 32, (size_t)wpb32 * st32>>>(A); ++launches;
                         CK(cudaGetLastError());
                     }
                     k_flip<<<(nb + 255) / 256, 256>>>(ddirs, dgeo, nb, 1, ddirpass, dretry); ++launches;
                     // FP64 pass over everything still pending
                     int grid = 0;
-                    CK(grid_for((const void *)k_search<double>, wpb64, st64, grid));
+                    CK(grid_for((const void *)ks64, wpb64, st64, grid));
                     A.n_warps = grid * wpb64; A.stage_bytes = st64;
                     A.ctl = dctl + 1; A.todo = dtodoall; A.n_todo = nb; A.pass = 2;
                     CK(cudaMemset(dready, 0, (size_t)q_cap * 4));
-                    k_search<double><<<grid, wpb64 * 32, (size_t)wpb64 * st64>>>(A); ++launches;
+                    ks64<<<grid, wpb64 * 32, (size_t)wpb64 * st64>>>(A); ++launches;
                     CK(cudaGetLastError());
                 }
             }

@@ -217,6 +217,9 @@ __device__ unsigned long long pfg_search_cycles[16];
 #endif
 
 // Per-lane register state: levels lane (slot 0) and lane + 32 (slot 1).
+// The search code is instantiated for NS = 1 slot (h11 <= 32: every level
+// and column has its own lane, and slot 1 is never touched, so the compiler
+// drops its registers) and NS = 2 (h11 up to 64).
 template <class R> struct Lanes {
     int64_t cur0, cur1, hi0, hi1;
     R rem0, rem1, err0, err1, off0, off1, aoff0, aoff1;
@@ -227,22 +230,22 @@ template <class R> struct Lanes {
     int64_t k0, k1;               // (ZB c)_r over c[1:]
 };
 
-#define LGET(S, f, i) shfl((i) < 32 ? S.f##0 : S.f##1, (i) & 31)
-#define LSET(S, f, i, val) do { if (lane == ((i) & 31)) { if ((i) < 32) S.f##0 = (val); else S.f##1 = (val); } } while (0)
+#define LGET(S, f, i) shfl((NS > 1 && (i) >= 32) ? S.f##1 : S.f##0, (i) & 31)
+#define LSET(S, f, i, val) do { if (lane == ((i) & 31)) { if (NS > 1 && (i) >= 32) S.f##1 = (val); else S.f##0 = (val); } } while (0)
 
 // c[i] changes by dv (i >= 1): update the exact incremental sums
-template <class R> __device__ __forceinline__ void apply_dc(Lanes<R> &S, const Prob<R> &P, int i, int64_t dv, int lane)
+template <class R, int NS> __device__ __forceinline__ void apply_dc(Lanes<R> &S, const Prob<R> &P, int i, int64_t dv, int lane)
 {
     if (dv == 0 || i == 0) return;
     const int d = P.d, h = P.h;
     if (lane < d) S.y0 += (int64_t)P.MAT[i * d + lane] * dv;
-    if (lane + 32 < d) S.y1 += (int64_t)P.MAT[i * d + lane + 32] * dv;
+    if (NS > 1 && lane + 32 < d) S.y1 += (int64_t)P.MAT[i * d + lane + 32] * dv;
     if (lane < h) S.k0 += (int64_t)P.ZT[i * h + lane] * dv;
-    if (lane + 32 < h) S.k1 += (int64_t)P.ZT[i * h + lane + 32] * dv;
+    if (NS > 1 && lane + 32 < h) S.k1 += (int64_t)P.ZT[i * h + lane + 32] * dv;
 }
 
 // the dot products of entering level i (c[i+1:] set): off, aoff, GCD prefix
-template <class R> __device__ __forceinline__ void level_sums(const Lanes<R> &S, const Prob<R> &P, int i, int lane,
+template <class R, int NS> __device__ __forceinline__ void level_sums(const Lanes<R> &S, const Prob<R> &P, int i, int lane,
                                                               R &off, R &aoff, i128 &pre)
 {
     const int d = P.d;
@@ -257,7 +260,7 @@ template <class R> __device__ __forceinline__ void level_sums(const Lanes<R> &S,
         if (hrow) pr += (i128)P.H[i * d + j] * S.c0;
     }
     j = lane + 32;
-    if (j > i && j < d) {
+    if (NS > 1 && j > i && j < d) {
         R t = Ui[j] * (R)S.c1;
         o += t; a += fabs(t);
         if (hrow) pr += (i128)P.H[i * d + j] * S.c1;
@@ -316,12 +319,25 @@ template <class R> __device__ __forceinline__ int level_range(const Prob<R> &P, 
 // the owner lanes' registers (kept for the return to this level and for
 // donation), and to the caller (every lane).  Returns ST_RANGE if a bound
 // leaves int32.
-template <class R> __device__ int enter_level(Lanes<R> &S, const Prob<R> &P, int i, R rem, R err, u128 gab,
+template <class R, int NS> __device__ int enter_level(Lanes<R> &S, const Prob<R> &P, int i, R rem, R err, u128 gab,
                                               int lane, int64_t &lo_o, int64_t &hi_o, R &off, R &aoff, i128 &pre)
 {
-    level_sums(S, P, i, lane, off, aoff, pre);
+#ifdef PFG_STAGE_CLOCKS
+    const long long e0 = clock64();
+#endif
+    level_sums<R, NS>(S, P, i, lane, off, aoff, pre);
+#ifdef PFG_STAGE_CLOCKS
+    const long long e1 = clock64();
+#endif
     int64_t lo, hi;
     const int st = level_range(P, i, rem, err, gab, off, aoff, lo, hi);
+#ifdef PFG_STAGE_CLOCKS
+    __syncwarp();
+    if (lane == 0 && sizeof(R) == 8) {
+        atomicAdd(&pfg_search_cycles[12], (unsigned long long)(e1 - e0));
+        atomicAdd(&pfg_search_cycles[13], (unsigned long long)(clock64() - e1));
+    }
+#endif
     if (st) return st;
     LSET(S, cur, i, lo); LSET(S, hi, i, hi);
     LSET(S, rem, i, rem); LSET(S, err, i, err);
@@ -332,17 +348,17 @@ template <class R> __device__ int enter_level(Lanes<R> &S, const Prob<R> &P, int
 }
 
 // exact leaf data of the level-0 node (c[1:] set): q(c) = A0 + 2 c0 B0 + m00 c0^2
-template <class R> __device__ __forceinline__ void leaf_data(const Lanes<R> &S, const Prob<R> &P, int lane,
+template <class R, int NS> __device__ __forceinline__ void leaf_data(const Lanes<R> &S, const Prob<R> &P, int lane,
                                                              i128 &A0, int64_t &B0)
 {
     i128 part = 0;
     if (lane >= 1 && lane < P.d) part += (i128)S.c0 * S.y0;
-    if (lane + 32 < P.d) part += (i128)S.c1 * S.y1;
+    if (NS > 1 && lane + 32 < P.d) part += (i128)S.c1 * S.y1;
     A0 = warp_sum128(part);
     B0 = shfl(S.y0, 0);
 }
 
-template <class R>
+template <class R, int NS>
 __device__ int run_subtree(const SearchArgs &A, const Prob<R> &P, int pid, const WorkItem *it, Tally &T, int lane)
 {
     const int d = P.d, h = P.h;
@@ -361,21 +377,21 @@ __device__ int run_subtree(const SearchArgs &A, const Prob<R> &P, int pid, const
     if (!it) {                                    // the root of the direction
         top = i = d - 1;
         u_rem = P.qmax_r; u_err = P.Kerr * P.qmax_r; u_gab = 0;
-        int st = enter_level(S, P, i, u_rem, u_err, u_gab, lane, u_cur, u_hi, u_off, u_aoff, u_pre);
+        int st = enter_level<R, NS>(S, P, i, u_rem, u_err, u_gab, lane, u_cur, u_hi, u_off, u_aoff, u_pre);
         if (st) return st;
         T.nodes++;
     } else {                                      // a donated node
         top = i = it->level;
         if (lane > i && lane < d) S.c0 = it->c[lane];
-        if (lane + 32 > i && lane + 32 < d) S.c1 = it->c[lane + 32];
+        if (NS > 1 && lane + 32 > i && lane + 32 < d) S.c1 = it->c[lane + 32];
         // exact incremental sums from scratch
         for (int j = i + 1; j < d; ++j) {
-            int32_t cj = shfl(j < 32 ? S.c0 : S.c1, j & 31);
-            apply_dc(S, P, j, cj, lane);
+            int32_t cj = shfl((NS > 1 && j >= 32) ? S.c1 : S.c0, j & 31);
+            apply_dc<R, NS>(S, P, j, cj, lane);
         }
         R off, aoff;
         i128 pre;
-        level_sums(S, P, i, lane, off, aoff, pre);
+        level_sums<R, NS>(S, P, i, lane, off, aoff, pre);
         const u128 gab = ((u128)it->ghi << 64) | it->glo;
         LSET(S, cur, i, it->cur); LSET(S, hi, i, it->hi);
         LSET(S, rem, i, (R)it->rem); LSET(S, err, i, (R)it->err);
@@ -388,7 +404,7 @@ __device__ int run_subtree(const SearchArgs &A, const Prob<R> &P, int pid, const
     // leaf data for the current level-0 node: q(v) = A0 + 2 v B0 + m00 v^2
     i128 A0 = 0;
     int64_t B0 = 0;
-    if (i == 0) leaf_data(S, P, lane, A0, B0);
+    if (i == 0) leaf_data<R, NS>(S, P, lane, A0, B0);
     const int64_t m00 = (int64_t)P.MAT[0];
     unsigned poll = 0;
     const unsigned long long t0 = shfl(gtimer(), 0);
@@ -402,14 +418,14 @@ __device__ int run_subtree(const SearchArgs &A, const Prob<R> &P, int pid, const
 #endif
         if (u_cur > u_hi) {                       // backtrack
             int32_t ci = LGET(S, c, i);
-            if (ci) { apply_dc(S, P, i, -(int64_t)ci, lane); LSET(S, c, i, 0); }
+            if (ci) { apply_dc<R, NS>(S, P, i, -(int64_t)ci, lane); LSET(S, c, i, 0); }
             ++i;
             if (i <= top) {                       // the parent's values from its owner lane
                 u_cur = LGET(S, cur, i); u_hi = LGET(S, hi, i);
                 u_rem = LGET(S, rem, i); u_err = LGET(S, err, i);
                 u_off = LGET(S, off, i); u_aoff = LGET(S, aoff, i);
-                u_gab = shflu128(i < 32 ? S.gab0 : S.gab1, i & 31);
-                u_pre = shfl128(i < 32 ? S.pre0 : S.pre1, i & 31);
+                u_gab = shflu128((NS > 1 && i >= 32) ? S.gab1 : S.gab0, i & 31);
+                u_pre = shfl128((NS > 1 && i >= 32) ? S.pre1 : S.pre0, i & 31);
             }
 #ifdef PFG_STAGE_CLOCKS
             acc_bt += clock64() - k0;
@@ -431,7 +447,7 @@ __device__ int run_subtree(const SearchArgs &A, const Prob<R> &P, int pid, const
             if (hungry) {
                 // highest level j in (i, top] with candidates left
                 bool has0 = lane > i && lane <= top && S.cur0 <= S.hi0;
-                bool has1 = lane + 32 > i && lane + 32 <= top && S.cur1 <= S.hi1;
+                bool has1 = NS > 1 && lane + 32 > i && lane + 32 <= top && S.cur1 <= S.hi1;
                 unsigned b1 = __ballot_sync(FULL, has1), b0 = __ballot_sync(FULL, has0);
                 int j = b1 ? 32 + 31 - __clz(b1) : (b0 ? 31 - __clz(b0) : -1);
                 if (j >= 0) {
@@ -442,14 +458,14 @@ __device__ int run_subtree(const SearchArgs &A, const Prob<R> &P, int pid, const
                         WorkItem *dst = A.items + slot;
                         const int64_t jc = LGET(S, cur, j), jh = LGET(S, hi, j);
                         const R jr = LGET(S, rem, j), je = LGET(S, err, j);
-                        const u128 jg = shflu128(j < 32 ? S.gab0 : S.gab1, j & 31);
+                        const u128 jg = shflu128((NS > 1 && j >= 32) ? S.gab1 : S.gab0, j & 31);
                         if (lane == 0) {
                             dst->pid = pid; dst->level = j; dst->cur = jc; dst->hi = jh;
                             dst->rem = (double)jr; dst->err = (double)je;
                             dst->glo = (uint64_t)jg; dst->ghi = (uint64_t)(jg >> 64);
                         }
                         if (lane > j && lane < d) dst->c[lane] = S.c0;
-                        if (lane + 32 > j && lane + 32 < d) dst->c[lane + 32] = S.c1;
+                        if (NS > 1 && lane + 32 > j && lane + 32 < d) dst->c[lane + 32] = S.c1;
                         __threadfence();
                         __syncwarp();
                         if (lane == 0) { atomicExch(&A.ready[slot], 1); atomicAdd(&A.ctl->donated, 1ull); }
@@ -519,14 +535,14 @@ __device__ int run_subtree(const SearchArgs &A, const Prob<R> &P, int pid, const
             const R nr0 = shfl(nr, t0), en0 = shfl(en, t0);
             const u128 g0 = shflu128(gn, t0);
             const int32_t ci = LGET(S, c, i);
-            apply_dc(S, P, i, vc - ci, lane);
+            apply_dc<R, NS>(S, P, i, vc - ci, lane);
             LSET(S, c, i, (int32_t)vc);
             --i;
             u_rem = nr0; u_err = en0; u_gab = g0;
-            int st = enter_level(S, P, i, u_rem, u_err, u_gab, lane, u_cur, u_hi, u_off, u_aoff, u_pre);
+            int st = enter_level<R, NS>(S, P, i, u_rem, u_err, u_gab, lane, u_cur, u_hi, u_off, u_aoff, u_pre);
             if (st) return st;
             T.nodes++;
-            if (i == 0) leaf_data(S, P, lane, A0, B0);
+            if (i == 0) leaf_data<R, NS>(S, P, lane, A0, B0);
 #ifdef PFG_STAGE_CLOCKS
             acc_ds += clock64() - k1;
 #endif
@@ -551,7 +567,7 @@ __device__ int run_subtree(const SearchArgs &A, const Prob<R> &P, int pid, const
             const i128 qt = shfl128(q, t);
             uint64_t g = 0;
             if (lane >= 1 && lane < h) g = gcd64(g, uabs64(S.k0 + (int64_t)P.ZT[lane] * vt));
-            if (lane + 32 < h) g = gcd64(g, uabs64(S.k1 + (int64_t)P.ZT[lane + 32] * vt));
+            if (NS > 1 && lane + 32 < h) g = gcd64(g, uabs64(S.k1 + (int64_t)P.ZT[lane + 32] * vt));
             for (int o = 16; o; o >>= 1) g = gcd64(g, __shfl_xor_sync(FULL, g, o));
             if (g != 0 && (i128)P.Q * (i128)g <= qt && lane == t) ok = false;
         }
@@ -580,7 +596,7 @@ __device__ int run_subtree(const SearchArgs &A, const Prob<R> &P, int pid, const
             int32_t *cc = A.coords + slot * MD;
             if (lane == 0) cc[0] = (int32_t)vt;
             else if (lane < d) cc[lane] = S.c0;
-            if (lane + 32 < d) cc[lane + 32] = S.c1;
+            if (NS > 1 && lane + 32 < d) cc[lane + 32] = S.c1;
         }
 #ifdef PFG_STAGE_CLOCKS
         PFG_SCLK(c_leaf_end);
@@ -620,11 +636,15 @@ static unsigned char emu_stage[64 * 1024];
 #define PFG_STAGE_AREA(A) ((void *)(pfg_stage_smem + (threadIdx.x >> 5) * (A).stage_bytes))
 #endif
 
-// Blocks of at most SEARCH_WARPS warps, three per SM: the search's registers
-// (about 165 per thread) then fit without spilling to local memory.
+// Blocks of at most SEARCH_WARPS warps, SEARCH_BLOCKS(NS) per SM: the
+// search's registers then fit without spilling to local memory.
 constexpr int SEARCH_WARPS = 4;
-template <class R>
-__global__ void __launch_bounds__(SEARCH_WARPS * 32, 3) k_search(SearchArgs A)
+#ifndef PFG_SEARCH_BLOCKS1
+#define PFG_SEARCH_BLOCKS1 4
+#endif
+template <int NS> constexpr int search_blocks() { return NS == 1 ? PFG_SEARCH_BLOCKS1 : 3; }
+template <class R, int NS>
+__global__ void __launch_bounds__(SEARCH_WARPS * 32, search_blocks<NS>()) k_search(SearchArgs A)
 {
 #ifndef PFG_EMU
     extern __shared__ __align__(16) unsigned char pfg_stage_smem[];
@@ -692,7 +712,7 @@ __global__ void __launch_bounds__(SEARCH_WARPS * 32, 3) k_search(SearchArgs A)
         if (lane == 0) pending = ((volatile Dir *)A.dirs)[pid].status == ST_PENDING;
         if (shfl(pending, 0)) {                   // (skip work of a direction that already failed)
             const Prob<R> P = load_prob<R>(A, pid, stage, lane);
-            st = run_subtree<R>(A, P, pid, it, T, lane);
+            st = run_subtree<R, NS>(A, P, pid, it, T, lane);
         }
 #ifdef PFG_STAGE_CLOCKS
         PFG_SCLK(c_end);
@@ -708,7 +728,7 @@ __global__ void __launch_bounds__(SEARCH_WARPS * 32, 3) k_search(SearchArgs A)
 
 // The plain form: one warp (block) per direction, no work sharing; pid < 0
 // takes the block's direction todo[blockIdx.x].
-template <class R>
+template <class R, int NS>
 __global__ void __launch_bounds__(32) k_search_plain(SearchArgs A, int pid)
 {
     if (pid < 0) {
@@ -725,7 +745,7 @@ __global__ void __launch_bounds__(32) k_search_plain(SearchArgs A, int pid)
     if (lane == 0) pending = A.dirs[pid].status == ST_PENDING;
     if (!shfl(pending, 0)) return;
     const Prob<R> P = load_prob<R>(A, pid, stage, lane);
-    int st = run_subtree<R>(A, P, pid, nullptr, T, lane);
+    int st = run_subtree<R, NS>(A, P, pid, nullptr, T, lane);
     finish_item<R>(A, pid, st, T, lane);
 }
 

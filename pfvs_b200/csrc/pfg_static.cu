@@ -112,7 +112,7 @@ __global__ void __launch_bounds__(32) k_direction_static(StaticScratch *S, int h
         Tally T{0, 0, 0};
         static_assert(sizeof(StaticScratch::stage) >= 49664, "staging area");
         const Prob<double> P = load_prob<double>(A, 0, S->stage, lane);
-        st = run_subtree<double>(A, P, 0, nullptr, T, lane);
+        st = run_subtree<double, 2>(A, P, 0, nullptr, T, lane);
         npts = shfl(S->ctl.npts, 0);
         if (st == 0 && npts > (unsigned long long)cap) st = -2;   // more points than the caller's buffers
         if (st == 0 && npts > (unsigned long long)STATIC_MAX_POINTS) st = -2;

@@ -96,9 +96,13 @@ extern "C" int emu_coni_batch(const pfg_input *in, int precision, int n_warps, p
     A.ready = ready.data(); A.q_cap = q_cap; A.hdr = hdr.data(); A.coords = coords.data();
     A.pts_cap = pts_cap; A.npts = &ctl[0].npts; A.dir_nodes = dnodes.data(); A.eps = 1e-4;
     A.donate = 1; A.n_warps = n_warps; A.wait_ns = 30ll * 1000000000ll; A.deadline_ns = 600ll * 1000000000ll;
+    // the device's choice of instantiation: one slot per lane when every h11 <= 32
+    int hmax = 3;
+    for (int k = 0; k < nb; ++k) hmax = std::max(hmax, geos[pgeo[k]].h);
+    const bool one = hmax <= 32;
     if (!todo32.empty()) {
         A.ctl = &ctl[0]; A.todo = todo32.data(); A.n_todo = (int)todo32.size(); A.pass = 1;
-        launch(n_warps, [&] { k_search<float>(A); });
+        launch(n_warps, [&] { if (one) k_search<float, 1>(A); else k_search<float, 2>(A); });
     }
     for (int pid = 0; pid < nb; ++pid) {          // k_flip
         Dir &D = dirs[pid];
@@ -108,7 +112,7 @@ extern "C" int emu_coni_batch(const pfg_input *in, int precision, int n_warps, p
     }
     std::fill(ready.begin(), ready.end(), 0);
     A.ctl = &ctl[1]; A.todo = todoall.data(); A.n_todo = nb; A.pass = 2;
-    launch(n_warps, [&] { k_search<double>(A); });
+    launch(n_warps, [&] { if (one) k_search<double, 1>(A); else k_search<double, 2>(A); });
     if (ctl[0].err || ctl[1].err) { snprintf(out->err, sizeof out->err, "wait ran out"); return 1; }
     const unsigned long long npts = ctl[0].npts;
     if (npts > pts_cap) { snprintf(out->err, sizeof out->err, "point buffer overflow"); return 1; }
