@@ -139,7 +139,7 @@ template <class R> struct Prob {
     int d, h, m0_level, pad;
     int64_t g_lin, Q, qmax, linmin;
     uint64_t hrows;
-    R qmax_r, slack, Kerr, max_err;
+    R qmax_r, slack, Kerr, max_err, invQ;
 };
 
 // Set up the problem of direction pid and stage its data in `stage` (the
@@ -178,14 +178,17 @@ template <class R> __device__ Prob<R> load_prob(const SearchArgs &A, int pid, vo
     P.slack = sl + (R)D.slack_chol;
     P.Kerr = (R)2 * (R)(D.d + 8) * Num<R>::U();
     P.max_err = sizeof(R) < sizeof(double) ? (R)1 + (R)0.05 * qd : (R)INFINITY;
+    P.invQ = (R)1 / (R)g.Q;
     return P;
 }
 
-// smallest gcd that can pass the GCD cut when q >= q_lb (fpk_search_impl.h:43-51)
-template <class R> __device__ __forceinline__ uint64_t need_of(R q_lb, int64_t Q)
+// smallest gcd that can pass the GCD cut when q >= q_lb (fpk_search_impl.h:43-51);
+// q_lb / Q as a product with the rounded 1/Q: its few units of rounding are far
+// inside the G (1 + t) margin taken off below
+template <class R> __device__ __forceinline__ uint64_t need_of(R q_lb, R invQ)
 {
     if (!(q_lb > 0)) return 0;
-    R t = q_lb / (R)Q;
+    R t = q_lb * invQ;
     t -= Num<R>::G() * ((R)1 + t);
     if (t < 0) t = 0;
     if (t >= (R)1.8e19) return UINT64_MAX;
@@ -417,8 +420,9 @@ __device__ int run_subtree(const SearchArgs &A, const Prob<R> &P, int pid, const
         const long long k0 = clock64();
 #endif
         if (u_cur > u_hi) {                       // backtrack
-            int32_t ci = LGET(S, c, i);
-            if (ci) { apply_dc<R, NS>(S, P, i, -(int64_t)ci, lane); LSET(S, c, i, 0); }
+            // (c[i] keeps its last value: nothing reads it or its share of
+            // the incremental sums until the next descent to level i, which
+            // applies the change from it)
             ++i;
             if (i <= top) {                       // the parent's values from its owner lane
                 u_cur = LGET(S, cur, i); u_hi = LGET(S, hi, i);
@@ -505,7 +509,7 @@ __device__ int run_subtree(const SearchArgs &A, const Prob<R> &P, int pid, const
                 else {
                     u128 a = uabs(pre + (i128)hii * v);
                     if ((gn >> 64) == 0 && (a >> 64) == 0 && (gn | a) != 0) {
-                        uint64_t gg = gcd64_ge_small((uint64_t)gn, (uint64_t)a, need_of(q_lb, P.Q));
+                        uint64_t gg = gcd64_ge_small((uint64_t)gn, (uint64_t)a, need_of(q_lb, P.invQ));
                         if (!gg) pass = false;
                         gn = gg;
                     } else {
