@@ -39,15 +39,15 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-# Roofline of the dominant kernel, k_search<double> (the persistent
-# FP64-pruned search, about 38 % of the launch list): scalar integer / FP64
+# Roofline of the dominant kernel, k_search<double, 1> (the persistent
+# FP64-pruned search, about 33 % of the launch list): scalar integer / FP64
 # warp code, neither HBM- nor tensor-bound, so its ceiling is the
 # warp-instruction issue rate, 148 SMs x 4 schedulers x SM clock.  Per-unit
 # figures from one ncu --set full capture of the timed form's search on the
 # first 16,384 directions of this batch (20,582,107 nodes): executed warp
 # instructions and DRAM bytes per search node.
-SEARCH_INST_PER_NODE = 17_437_909_937 / 20_582_107
-SEARCH_DRAM_PER_NODE = (244_797_696 + 107_985_664) / 20_582_107
+SEARCH_INST_PER_NODE = 14_977_918_824 / 20_582_107
+SEARCH_DRAM_PER_NODE = (248_137_216 + 110_171_648) / 20_582_107
 # The setup's three phase kernels (k_setup<32, 0..2>) together, from the
 # same kind of capture on the same 16,384 directions: per direction.
 SETUP_INST_PER_DIR = (3_785_943_035 + 6_529_456_061 + 1_841_800_499) / 16384
@@ -348,7 +348,7 @@ def main():
         del Kp, Mp, pp
     # roofline of the search kernel: executed warp instructions per launch (ncu
     # per-node figure x the launch's nodes) over its CUDA-event time (the
-    # search stage: k_flip, a few microseconds, then k_search<double>); the
+    # search stage: k_flip, a few microseconds, then k_search<double, 1>); the
     # setup's three phase kernels beside it, per direction
     peaks, peaks_kind = measured_peaks()
     clk_sum = clk.summary()
@@ -356,7 +356,7 @@ def main():
     peak = N_SM * SCHEDULERS * mhz * 1e6
     search_s = stats["ms_search"] / 1e3
     achieved = SEARCH_INST_PER_NODE * stats["nodes"] / search_s
-    roofline = {"kernel": "k_search<double>", "bound": "issue", "achieved": achieved, "peak": peak,
+    roofline = {"kernel": "k_search<double, 1>", "bound": "issue", "achieved": achieved, "peak": peak,
                 "unit": "warp-inst/s", "frac": achieved / peak,
                 "traffic": SEARCH_DRAM_PER_NODE * stats["nodes"],
                 "basis": f"ncu: {SEARCH_INST_PER_NODE:.0f} warp-inst and {SEARCH_DRAM_PER_NODE:.1f} DRAM bytes per "
