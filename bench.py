@@ -219,6 +219,12 @@ def cpu_reference_run(geoms, ps, pgeo, threads, deadline_s=None):
     return dt, sum(r[0] for r in res), sum(r[1] for r in res), sum(r[2] for r in res)
 
 
+def workload_desc(args, w):
+    """The config's workload string (the same for both arms)."""
+    return (f"{args.workload}: {len(w)} p-hat directions over {len(w.geoms)} geometries "
+            f"h11={[g.h11 for g in w.geoms]}, dilations {list(w.info.get('dilations', []))}")
+
+
 def run_reference(args, world, rank, pg):
     if rank != 0:
         return
@@ -247,8 +253,9 @@ def run_reference(args, world, rank, pg):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int64",
             "data": "synthetic (seeded)",
-            "config": {"workload": f"{args.workload} sample of {len(pick)} directions "
-                                   f"(random, seed 1) of {len(w)}", "threads": threads},
+            "config": {"workload": workload_desc(args, w),
+                       "sample": f"{len(pick)} random directions (seed 1) of the batch per step",
+                       "threads": threads},
             "directions_per_s": dirs / t, "points_per_s": pts / t,
             "cpu_baseline": {"value": v, "unit": "nodes/s", "cores": threads, "kind": "reference",
                              "sample": f"{len(pick)} directions of the {args.workload} batch; "
@@ -373,11 +380,10 @@ def main():
         line = {"metric": "lattice nodes/s", "value": value, "unit": "nodes/s", "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup,
                 "ms_per_step": dev_s / args.steps * 1e3, "higher_is_better": True,
-                "scaling": "weak", "vs_baseline": None, "dtype": "int64+fp32",
+                "scaling": "weak", "vs_baseline": None,
+                "dtype": "int64+fp32" if args.precision == "fp32" else "int64+fp64",
                 "data": "synthetic (seeded CY instances, pfvs_b200/workloads.py)",
-                "config": {"workload": f"{args.workload}: {len(w)} p-hat directions over "
-                                       f"{len(w.geoms)} geometries h11={[g.h11 for g in w.geoms]}, "
-                                       f"dilations {list(w.info.get('dilations', []))}",
+                "config": {"workload": workload_desc(args, w),
                            "form": args.form, "precision": args.precision,
                            "directions_per_gpu": len(idx),
                            "l2": "working set per step > 126 MB (slabs + points); no flush needed",
@@ -386,7 +392,7 @@ def main():
                 "directions_per_s": allsum(pg, len(idx)) * args.steps / dev_s,
                 "stage_ms": {"setup": stats["ms_setup"], "search": stats["ms_search"],
                              "output": stats["ms_output"]},
-                "fp32_nodes_per_step": stats["nodes"], "wall_ms_per_step": wall_s / args.steps * 1e3,
+                "timed_form_nodes_per_step": stats["nodes"], "wall_ms_per_step": wall_s / args.steps * 1e3,
                 "clocks": clk_sum, "e2e": e2e, "cpu_baseline": cpu, "roofline": roofline, "roofline_setup": roofline_setup, "pfvs": pfv,
                 "gpu_launches": int(stats.get("launches", 0)) * args.steps}
         print(json.dumps(line))
