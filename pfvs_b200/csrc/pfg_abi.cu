@@ -429,7 +429,7 @@ static int coni_run(const pfg_input *in, const pfg_options *opt_in, pfg_output *
             while (n32 < nb && geos[in->pgeo[off + order[n32]]].h <= 32) ++n32;
             const int n64 = nb - n32;
             const size_t smem32 = sizeof(LllMem<32>);
-            int grid32 = 0, grid64 = 0;
+            int grid32 = 0, grid64[3] = {0, 0, 0};
             if (n32) {
                 CK(cudaFuncSetAttribute(k_setup<32, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem32));
                 CK(cudaFuncSetAttribute(k_setup<32, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem32));
@@ -438,8 +438,18 @@ static int coni_run(const pfg_input *in, const pfg_options *opt_in, pfg_output *
                 CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bpsm, k_setup<32, 1>, 32, smem32));
                 grid32 = std::min(n32, nsm * std::max(1, bpsm));
             }
-            if (n64) grid64 = std::min((n64 + 3) / 4, nsm * 2);
-            const int setup_warps = std::max(grid32, grid64 * 4);
+            if (n64) {
+                // the global-scratch LLL is latency-bound: as many blocks per SM as each phase's
+                // registers allow
+                const void *f64[3] = {(const void *)k_setup<MH, 0>, (const void *)k_setup<MH, 1>,
+                                      (const void *)k_setup<MH, 2>};
+                for (int p = 0; p < 3; ++p) {
+                    int bpsm = 0;
+                    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bpsm, f64[p], 128, 0));
+                    grid64[p] = std::min((n64 + 3) / 4, nsm * std::max(1, bpsm));
+                }
+            }
+            const int setup_warps = std::max(grid32, 4 * std::max(grid64[0], std::max(grid64[1], grid64[2])));
             WS(dps, W_PS, (size_t)nb * MH * 8);
             WS(dpgeo, W_PGEO, (size_t)nb * 4);
             WS(dslaboff, W_SLABOFF, (size_t)nb * 8);
@@ -481,13 +491,13 @@ static int coni_run(const pfg_input *in, const pfg_options *opt_in, pfg_output *
                 SetupArgs SA64{dgeo, dkappa, dmb, dps, dpgeo, dslaboff, dslab, ddirs, dscr, n64,
                                counters + 3, dorder + n32, 0, gcd_min_tree};
                 if (n32) { k_setup<32, 0><<<grid32, 32, smem32>>>(SA32); ++launches; }
-                if (n64) { k_setup<MH, 0><<<grid64, 128>>>(SA64); ++launches; }
+                if (n64) { k_setup<MH, 0><<<grid64[0], 128>>>(SA64); ++launches; }
                 SA32.next = counters + 1; SA64.next = counters + 4;
                 if (n32) { k_setup<32, 1><<<grid32, 32, smem32>>>(SA32); ++launches; }
-                if (n64) { k_setup<MH, 1><<<grid64, 128>>>(SA64); ++launches; }
+                if (n64) { k_setup<MH, 1><<<grid64[1], 128>>>(SA64); ++launches; }
                 SA32.next = counters + 2; SA64.next = counters + 5;
                 if (n32) { k_setup<32, 2><<<grid32, 32, smem32>>>(SA32); ++launches; }
-                if (n64) { k_setup<MH, 2><<<grid64, 128>>>(SA64); ++launches; }
+                if (n64) { k_setup<MH, 2><<<grid64[2], 128>>>(SA64); ++launches; }
                 CK(cudaGetLastError());
             }
             CK(cudaEventRecord(ev[1]));
