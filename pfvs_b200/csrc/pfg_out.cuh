@@ -139,10 +139,19 @@ __global__ void k_keys(OutArgs O, unsigned long long n_kept)
         const int32_t *c = O.coords + (unsigned long long)k * MD;
         const int32_t c0 = lane < d ? c[lane] : 0, c1 = lane + 32 < d ? c[lane + 32] : 0;
         int64_t m0 = 0, m1 = 0;
-        for (int a = 0; a < d; ++a) {
-            const int64_t ca = __shfl_sync(FULL, a < 32 ? c0 : c1, a & 31);
-            if (lane < h) m0 += (int64_t)(int32_t)BT[a * h + lane] * ca;
-            if (lane + 32 < h) m1 += (int64_t)(int32_t)BT[a * h + lane + 32] * ca;
+        if (h <= 32) {                                  // (warp-uniform) one column per lane
+            const int64_t *col = BT + (lane < h ? lane : 0);
+            for (int a = 0; a < d; ++a) {
+                const int32_t ca = __shfl_sync(FULL, c0, a);
+                m0 += (int64_t)(int32_t)col[a * h] * ca;
+            }
+            if (lane >= h) m0 = 0;
+        } else {
+            for (int a = 0; a < d; ++a) {
+                const int64_t ca = __shfl_sync(FULL, a < 32 ? c0 : c1, a & 31);
+                if (lane < h) m0 += (int64_t)(int32_t)BT[a * h + lane] * ca;
+                if (lane + 32 < h) m1 += (int64_t)(int32_t)BT[a * h + lane + 32] * ca;
+            }
         }
         int64_t *key = O.keys + t * O.ks;
         if (lane < h) key[lane] = m0;
@@ -299,10 +308,19 @@ __global__ void k_rows(RowArgs R)
         const int64_t *key = R.keys + (unsigned long long)R.krow[t] * R.ks;
         const int64_t m0 = lane < h ? key[lane] : 0, m1 = lane + 32 < h ? key[lane + 32] : 0;
         int64_t k0 = 0, k1 = 0;
-        for (int a = 0; a < d; ++a) {
-            const int64_t ca = __shfl_sync(FULL, a < 32 ? c0 : c1, a & 31);
-            if (lane < h) k0 += (int64_t)(int32_t)ZT[a * h + lane] * ca;
-            if (lane + 32 < h) k1 += (int64_t)(int32_t)ZT[a * h + lane + 32] * ca;
+        if (h <= 32) {                                  // (warp-uniform) one column per lane
+            const int64_t *col = ZT + (lane < h ? lane : 0);
+            for (int a = 0; a < d; ++a) {
+                const int32_t ca = __shfl_sync(FULL, c0, a);
+                k0 += (int64_t)(int32_t)col[a * h] * ca;
+            }
+            if (lane >= h) k0 = 0;
+        } else {
+            for (int a = 0; a < d; ++a) {
+                const int64_t ca = __shfl_sync(FULL, a < 32 ? c0 : c1, a & 31);
+                if (lane < h) k0 += (int64_t)(int32_t)ZT[a * h + lane] * ca;
+                if (lane + 32 < h) k1 += (int64_t)(int32_t)ZT[a * h + lane + 32] * ca;
+            }
         }
         int64_t *Mr = R.M + t * MH, *Kr = R.Kn + t * MH;
         Mr[lane] = m0; Mr[lane + 32] = m1;
