@@ -165,6 +165,30 @@ def matmul(A, B):
     return [[sum(a * b for a, b in zip(row, col)) for col in zip(*B)] for row in A]
 
 
+class NotPositiveDefinite(ValueError):
+    """The ellipsoid matrix is not positive definite: the reference's kernel
+    status -9 (fpk_common.h:259-309), which coniZpM raises as
+    IncompleteSearchError (coni.py:446-453)."""
+
+
+def is_positive_definite(mat):
+    """Sylvester's criterion, exactly: every leading principal minor of the
+    symmetric integer matrix is > 0 (fraction-free Bareiss elimination; the
+    pivots are the leading minors)."""
+    A = [[int(x) for x in r] for r in mat]
+    d = len(A)
+    prev = 1
+    for k in range(d):
+        pk = A[k][k]
+        if pk <= 0:
+            return False
+        for i in range(k + 1, d):
+            for j in range(k + 1, d):
+                A[i][j] = (pk * A[i][j] - A[i][k] * A[k][j]) // prev
+        prev = pk
+    return True
+
+
 def build(kappa, Mbasis, p):
     """
     Per-direction lattice data (pfl_build, coni, extra_lll, m0_basis).
@@ -188,6 +212,13 @@ def build(kappa, Mbasis, p):
     Binter = [[BT[order[a]][i] for a in range(d)] for i in range(h)]
     ZB = matmul(Z, Binter)
     mat = [[-sum(Binter[i][a] * ZB[i][b] for i in range(h)) for b in range(d)] for a in range(d)]
+    # A direction whose kappa.p lacks the signature (1, h11-1) gives an
+    # indefinite mat.  The reference's C setup fails on it (the LLL w.r.t.
+    # mat below meets a non-positive norm), its Python path rebuilds mat with
+    # the Euclidean reduction only, and the exact factorization then reports
+    # -9 (coni.py:1025-1046, fpk_common.h:259-309): decide that here.
+    if not is_positive_definite(mat):
+        raise NotPositiveDefinite("the ellipsoid matrix is not positive definite")
     # cut-aware basis change (pfv_lattice.h:554-602)
     l = Binter[0]
     if any(x != 0 for x in l):

@@ -147,7 +147,11 @@ def _gcd(a, b):
 def direction(kappa, Mbasis, p, Q, qmax, linmin, eps=1e-4, max_out=10**9, prune=True):
     """Setup + search + emission for one direction.  Returns
     (M (n,h), Kn (n,h), q (n,), status, nodes)."""
-    L = lattice.build(kappa, Mbasis, p)
+    try:
+        L = lattice.build(kappa, Mbasis, p)
+    except lattice.NotPositiveDefinite:
+        h = np.asarray(Mbasis).shape[0]
+        return (np.zeros((0, h), np.int64), np.zeros((0, h), np.int64), np.zeros(0, np.int64), -9, 0)
     h, d = L["h"], L["d"]
     B, ZB, mat = L["Binter"], L["ZB"], L["mat"]
     st, U, N, V, Va = lattice.factor(mat, B[0])

@@ -366,7 +366,7 @@ template <int N> PFG_NOINLINE __device__ int warp_lll(Lll<N> &L, int m, bool has
     PFG_COUNT(0, 1);
     if (m >= 1) {
         lll_gs(S, 0, lane);
-        if (!(S->bb[0] > 0)) return ST_OVERFLOW;
+        if (!(S->bb[0] > 0)) return ST_NONPOS;
     }
     if (m >= 2) lll_gs(S, 1, lane);
     int k = 1, iters = 0;
@@ -377,7 +377,7 @@ template <int N> PFG_NOINLINE __device__ int warp_lll(Lll<N> &L, int m, bool has
         const double bk = S->bb[k], mk = S->mu[mix(k, k - 1)], bk1 = S->bb[k - 1];
         PFG_UNIFORM(bk);
         __syncwarp();                       // (every lane has read them before lll_swap writes)
-        if (!(bk > 0)) return ST_OVERFLOW;
+        if (!(bk > 0)) return ST_NONPOS;
         if (bk < (delta - mk * mk) * bk1) {
             PFG_T0(t_s);
             lll_swap(L, k, lane);
@@ -589,6 +589,98 @@ PFG_NOINLINE __device__ int warp_unimodular(const int64_t *vin, int n, int64_t *
 #endif
 
 // ---------------------------------------------------------------------------
+// Exact proof that a symmetric integer matrix A (d x d, row-major) is NOT
+// positive definite, for the directions whose FP64 factorization fails.
+//
+// An FP64 Cholesky A = U^T U runs until a pivot fails (or, if none does, to
+// the pivot j with the smallest ratio pivot / A_jj).  With y the solution of
+// A[<j, <j] y = A[<j, j] through the computed factor, x = (-y, 1, 0, ..) has
+// x^T A x = A_jj - A[j, <j] y, the Schur complement the pivot estimates.  x
+// is scaled by a power of two D = 2^t and rounded to integers, and x^T A x
+// is evaluated exactly in int128.  A value <= 0 at the nonzero integer x
+// proves A is not positive definite -- the decision the reference's exact
+// Bareiss factorization reaches by a non-positive leading minor (status -9,
+// fpk_common.h:259-309; Sylvester's criterion).  Rounding only moves x^T A x
+// by O(D |x| |A|) against D^2 times the Schur complement, so a clearly
+// negative pivot always gives a witness.  Returns false when none is found:
+// A may still be indefinite with a pivot lost in rounding, or positive
+// definite and too ill-conditioned to certify.  U: d*d doubles, y: d doubles
+// of scratch (y is reused for the integer witness).
+// ---------------------------------------------------------------------------
+__device__ bool witness_not_pd(const int64_t *A, int d, double *U, double *y, int lane)
+{
+    int jw = -1;                                // the pivot the witness is built at
+    double rmin = 1.0;
+    for (int j = 0; j < d; ++j) {
+        if (A[j * d + j] <= 0) return true;     // e_j itself: e_j^T A e_j = A_jj <= 0
+        double s0 = 0.0;
+        for (int k = 0; k < j; ++k) { const double u = U[k * d + j]; s0 += u * u; }
+        const double ajj = (double)A[j * d + j], pj = ajj - s0;
+        if (!(pj > 0)) { jw = j; break; }
+        if (pj / ajj < rmin) { rmin = pj / ajj; jw = j; }
+        const double ujj = sqrt(pj);
+        for (int i = j + 1 + lane; i < d; i += 32) {
+            double s = 0.0;
+            for (int k = 0; k < j; ++k) s += U[k * d + j] * U[k * d + i];
+            U[j * d + i] = ((double)A[j * d + i] - s) / ujj;
+        }
+        if (lane == 0) U[j * d + j] = ujj;
+        __syncwarp();
+    }
+    PFG_UNIFORM(jw);
+    if (jw <= 0) return false;
+    const int j = jw, n = j + 1;
+    // z = U[<j, j] (the forward substitution U^T z = A[<j, j] is column j of
+    // U's first j rows), then U[<j, <j] y = z backwards
+    for (int i = j - 1; i >= 0; --i) {
+        double s = 0.0;
+        for (int k = i + 1 + lane; k < j; k += 32) s += U[i * d + k] * y[k];
+        s = warp_sum(s);
+        if (lane == 0) y[i] = (U[i * d + j] - s) / U[i * d + i];
+        __syncwarp();
+    }
+    double ymax = 1.0;
+    uint64_t amax = 1;
+    for (int i = lane; i < j; i += 32) ymax = fmax(ymax, fabs(y[i]));
+    for (int e = lane; e < n * n; e += 32) {
+        const uint64_t a = uabs64(A[(e / n) * d + e % n]);
+        amax = a > amax ? a : amax;
+    }
+    for (int o = 16; o; o >>= 1) {
+        ymax = fmax(ymax, __shfl_xor_sync(FULL, ymax, o));
+        const uint64_t t = __shfl_xor_sync(FULL, amax, o);
+        amax = t > amax ? t : amax;
+    }
+    if (!(ymax < 1e300)) return false;
+    // |x| < 2^xb with 2 xb + bits(amax) + 2 bits(n) <= 124 keeps every partial sum of
+    // x^T A x inside int128 (the checked arithmetic below still guards it)
+    const int bits_a = 64 - __clzll((long long)amax), bits_n = 32 - __clz(n);
+    const int xb = min(60, (124 - bits_a - 2 * bits_n) / 2);
+    int ey = 0;
+    frexp(ymax, &ey);                           // ymax < 2^ey
+    const int t = xb - ey - 1;
+    if (t < 0) return false;
+    const double D = ldexp(1.0, t);
+    int64_t *x = (int64_t *)y;
+    for (int i = lane; i < n; i += 32) x[i] = i < j ? (int64_t)llrint(-y[i] * D) : ((int64_t)1 << t);
+    __syncwarp();
+    bool bad = false;
+    i128 qf = 0;
+    for (int i = lane; i < n; i += 32) {
+        i128 r = 0, tt;
+        for (int k = 0; k < n; ++k)
+            if (mul_ovf((i128)A[i * d + k], (i128)x[k], &tt) || add_ovf(r, tt, &r)) bad = true;
+        if (mul_ovf(r, (i128)x[i], &tt) || add_ovf(qf, tt, &qf)) bad = true;
+    }
+    for (int o = 16; o; o >>= 1) {
+        const i128 other = shfl_xor_i128(qf, o);
+        if (add_ovf(qf, other, &qf)) bad = true;
+    }
+    if (warp_any(bad)) return false;
+    return qf <= 0;
+}
+
+// ---------------------------------------------------------------------------
 // The setup of one direction in three phases, each a kernel of its own in the
 // batched path so that the warps of an SM run the same code (the phases'
 // code together does not fit the instruction caches).  They share only the
@@ -653,7 +745,7 @@ template <int N> __device__ int setup_phase0(const SetupArgs &A, int pid, int la
     if (gram_euclid<N>(S, d, h, lane)) return ST_OVERFLOW;
     {
         Lll<N> LL{S, h, d};
-        if ((st = warp_lll(LL, d, false, PFG_DELTA_O, lane))) return st;
+        if ((st = warp_lll(LL, d, false, PFG_DELTA_O, lane))) return st == ST_NONPOS ? ST_OVERFLOW : st;
     }
     clk.mark(5);
     // 5. (Mbasis O^T)^T rows, 6. coni order (rows with entry 0 == 0 first, stable)
@@ -754,7 +846,13 @@ template <int N> __device__ int setup_phase1(const SetupArgs &A, int pid, int la
         if (warp_any(bad)) return ST_OVERFLOW;
         {
             Lll<N> LK{S, d, d};
-            if ((st = warp_lll(LK, d - 1, true, PFG_DELTA_K, lane))) return st;
+            if ((st = warp_lll(LK, d - 1, true, PFG_DELTA_K, lane))) {
+                // a non-positive norm under mat: not positive definite when an
+                // integer witness says so (exact), else not decided here
+                if (st == ST_NONPOS)
+                    st = witness_not_pd(MAT, d, W->X, W->X + d * d, lane) ? ST_NOT_PD : ST_PRECISION;
+                return st;
+            }
         }
         // new columns a of Binter: sum_b B[a][b] Binter[:, b]  (likewise ZB)
         for (int e = lane; e < d * h; e += 32) {
@@ -830,7 +928,8 @@ template <int N> __device__ int setup_phase2(const SetupArgs &A, int pid, int la
         if (lane == 0) U[j * d + j] = ujj;
         __syncwarp();
     }
-    if (notpd) return ST_PRECISION;          // not certified positive definite here
+    if (notpd)                               // not positive definite, or not decided here
+        return witness_not_pd(MAT, d, U, W->X, lane) ? ST_NOT_PD : ST_PRECISION;
     // ||U||_F^2 and ||U^-1||_F^2
     double *X = W->X;
     for (int j = 0; j < d; ++j) {
@@ -857,7 +956,8 @@ template <int N> __device__ int setup_phase2(const SetupArgs &A, int pid, int la
     f2 = warp_sum(f2);
     const double u = 0x1p-53, gam = (d + 1) * u / (1.0 - (d + 1) * u);
     const double K = 2.0 * f1 * f2;              // 2x for the rounding in computing f2
-    if (!(gam * K <= 1e-3)) return ST_PRECISION;
+    if (!(gam * K <= 1e-3))                  // ill-conditioned: maybe not positive definite
+        return witness_not_pd(MAT, d, U, W->X, lane) ? ST_NOT_PD : ST_PRECISION;
     const double slack_chol = 2.0 * gam * K * ((double)g.qmax + 1.0);
     float *U32 = (float *)(slab + L.u32);
     double *UI = (double *)(slab + L.ui64);

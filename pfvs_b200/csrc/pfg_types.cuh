@@ -25,6 +25,7 @@ enum : int {
     ST_OVERFLOW = -20,  // exact setup values beyond the device's fixed-width integers
     ST_PRECISION = -21, // FP64 factor not certified (ill-conditioned beyond bounds)
     ST_WAIT = -22,      // a bounded device wait ran out
+    ST_NONPOS = -30,    // (internal, never reported) a Gram-Schmidt norm <= 0 in an LLL
 };
 
 struct Geo {

@@ -36,6 +36,8 @@ def _load():
                                        ctypes.POINTER(ctypes.c_int32)]
         lib.emu_coni_batch.restype = ctypes.c_int
         lib.emu_output_free.argtypes = [ctypes.POINTER(gpu._Output)]
+        lib.emu_witness_not_pd.argtypes = [ctypes.POINTER(ctypes.c_int64), ctypes.c_int]
+        lib.emu_witness_not_pd.restype = ctypes.c_int
         _lib = lib
     return _lib
 
@@ -69,3 +71,11 @@ def coni_batch_multi(geoms, ps, pgeo, precision=2, n_warps=2):
     finally:
         lib.emu_output_free(ctypes.byref(out))
     return M, Kn, q, pidx, pstat, dn[:n_p], dbg[:n_p]
+
+
+def witness_not_pd(A):
+    """The setup's exact witness that the symmetric integer matrix A is not
+    positive definite (True: proved indefinite; False: no witness found)."""
+    lib = _load()
+    A = np.ascontiguousarray(A, dtype=np.int64)
+    return bool(lib.emu_witness_not_pd(A.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)), A.shape[0]))

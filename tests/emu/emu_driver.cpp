@@ -161,3 +161,17 @@ extern "C" void emu_output_free(pfg_output *out)
     free(out->M); free(out->Kn); free(out->q); free(out->pidx); free(out->pstat);
     memset(out, 0, sizeof *out);
 }
+
+// The setup's exact non-positive-definiteness witness (pfg_setup.cuh,
+// witness_not_pd) on one emulated warp, for a d x d symmetric integer matrix:
+// 1 if it proves A is not positive definite, else 0.
+extern "C" int emu_witness_not_pd(const int64_t *A, int d)
+{
+    std::vector<double> U((size_t)d * d + 1), y((size_t)d + 1);
+    int res = 0;
+    emu_run_warp(0, 0, 32, 1, [&] {
+        const bool w = witness_not_pd(A, d, U.data(), y.data(), threadIdx.x & 31);
+        if ((threadIdx.x & 31) == 0) res = w ? 1 : 0;
+    });
+    return res;
+}
