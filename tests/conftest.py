@@ -7,7 +7,8 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 if ROOT not in sys.path:
     sys.path.insert(0, ROOT)
 
-REFERENCE = "/root/reference"
+# the reference tree (read only by CPU tests that need it; absent on GPU machines)
+REFERENCE = os.environ.get("PFVS_REFERENCE", "/root/reference")
 
 
 def pytest_configure(config):

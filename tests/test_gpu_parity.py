@@ -48,8 +48,8 @@ def test_batched_matches_oracle(case):
     assert_same(got, exp)
 
 
-@pytest.mark.parametrize("case", CASES[:6], ids=[_ids(c) for c in CASES[:6]])
-def test_batched_matches_reference_build(case, ref_available):
+@pytest.mark.parametrize("case", CASES, ids=[_ids(c) for c in CASES])
+def test_batched_matches_reference_build(case, ref_available, record_property):
     if not ref_available:
         pytest.skip("oracle/_ref not built")
     name, n, dils = case
@@ -58,7 +58,9 @@ def test_batched_matches_reference_build(case, ref_available):
     got = gpu.coni_batch_multi(geoms, ps, pgeo)
     exp = expected(geoms, ps, pgeo, "ref")
     ok = exp[4] == 0            # (directions the reference's C path finished)
-    assert ok.mean() > 0.5
+    record_property("finished_by_reference_build", float(ok.mean()))
+    print(f"{_ids(case)}: reference build finished {ok.mean():.4f} of {len(ok)} directions")
+    assert ok.mean() >= 0.9
     assert_same(got, exp, ok_mask=ok)
 
 
