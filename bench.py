@@ -5,26 +5,35 @@ Workload: the "mixed" synthetic batch -- 4 Calabi-Yau geometries with
 h11 in {8, 16, 24, 32} (h21 = 2 h11 + 40), 65,536 p-hat directions with
 entries in [1, 10], dilation per direction from {1, 2, 3, 4}
 (pfvs_b200/workloads.py).  A step is one pass of the pipeline over the whole
-batch: per-direction lattice setup, FP32-pruned search (FP64 retry on -11)
-and the canonical output, in one multi-geometry call.
+batch: per-direction lattice setup, the persistent search with the library's
+default pruning (FP64 on B200; --precision fp32 gives the FP32-pruned form
+with its FP64 retry on -11) and the canonical output, in one
+multi-geometry call.
 
 Metric: lattice nodes/s.  A node is one search-tree node entered; the work
 unit of the batch is the node count of its FP64-pruned tree (counted once,
-untimed), so FP32's extra nodes are not counted.  PFVs/s is reported beside
-it (points -> (K, M) PFVs by the exact post-processing).
+untimed), so FP32's extra nodes are not counted.  Directions/s and points/s
+are printed beside it in both arms (units the reference counts the same way).
 
 - value: device time of the K timed steps (CUDA events on the launching
   stream inside the library, inputs resident), nodes / time.
-- e2e:  the same metric through the public C-ABI entry point pfg_coni_batch
-  with host buffers (inputs copied in, points copied out every step),
-  wall clock around the K calls.
+- e2e:  the same metric through the library's public entry point
+  (pfvs_b200.gpu.coni_batch_multi -> the C ABI) with host buffers (inputs
+  copied in, points copied out every step), wall clock around the K calls.
+- failed_directions: directions the device did not finish, by status
+  (none on the benchmark's workloads).
 - cpu_baseline: the reference's own CPU kernel (oracle/_ref, compiled from
-  its sources) on a bounded sample of the batch, all host cores.
-- --impl reference: that CPU kernel as the timed arm.
+  its sources) over the whole batch once, on all host threads.
+- --impl reference: that CPU kernel as the timed arm: the K steps cover the
+  batch exactly once (step k takes the k-th of K disjoint slices), so the
+  arm times the same directions as this one.
+- plain / fp32 forms and PFVs/s: see `extras` below.
 
-Multi-GPU: directions are independent, so each rank takes a contiguous
-1/N of the batch (weak scaling: the batch grows with N), no collective on
-the data path; timing is the max over ranks.
+Multi-GPU: directions are independent.  The batch has N x 65,536
+directions (weak scaling), cut into contiguous chunks that the ranks pull
+from one shared queue (the process group's store: dynamic balancing, as the
+tree sizes differ by more than 1000x); no collective on the data path, the
+chunks' points concatenate in p order; timing is the max over ranks.
 """
 import argparse
 import json
@@ -73,9 +82,11 @@ def parse():
     ap.add_argument("--n", type=int, default=0, help="directions per GPU (0: the workload's size)")
     ap.add_argument("--form", default="batched", choices=["batched", "plain"])
     ap.add_argument("--precision", default="auto", choices=["auto", "fp64", "fp32"])
-    ap.add_argument("--cpu-sample", type=int, default=0, help="directions in the CPU sample (0: auto)")
+    ap.add_argument("--cpu-sample", type=int, default=0, help="directions in the CPU baseline (0: the whole batch)")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-extras", action="store_true", help="skip the forms and PFV figures")
+    ap.add_argument("--chunk", type=int, default=8192, help="directions per queue chunk (N > 1)")
     return ap.parse_args()
 
 
@@ -162,12 +173,12 @@ class Clocks:
                 "samples": len(self.samples)}
 
 
-def workload_slice(name, n_total, rank, world):
+def workload_for(name, n_per_gpu, world):
+    """The benchmark batch: n_per_gpu directions (0: the workload's own size)
+    for each of the `world` GPUs (weak scaling), the same on every rank."""
     from pfvs_b200 import workloads
-    w = workloads.build(name, n_p=n_total)
-    per = (len(w) + world - 1) // world
-    lo, hi = rank * per, min(len(w), (rank + 1) * per)
-    return w, list(range(lo, hi))
+    n = (n_per_gpu or workloads.SPECS[name][1]) * world
+    return workloads.build(name, n_p=n)
 
 
 def layout(w, idx):
@@ -219,6 +230,12 @@ def cpu_reference_run(geoms, ps, pgeo, threads, deadline_s=None):
     return dt, sum(r[0] for r in res), sum(r[1] for r in res), sum(r[2] for r in res)
 
 
+def failed_by_status(pstat):
+    """{status: directions} of the directions the device did not finish."""
+    st, n = np.unique(np.asarray(pstat)[np.asarray(pstat) != 0], return_counts=True)
+    return {int(a): int(b) for a, b in zip(st, n)}
+
+
 def workload_desc(args, w):
     """The config's workload string (the same for both arms)."""
     return (f"{args.workload}: {len(w)} p-hat directions over {len(w.geoms)} geometries "
@@ -234,34 +251,105 @@ def run_reference(args, world, rank, pg):
         print(json.dumps({"impl": "reference", "metric": metric,
                           "unavailable": "oracle/_ref (the reference CPU kernel) is not built"}))
         return
-    w, idx = workload_slice(args.workload, args.n or None, 0, 1)
+    w = workload_for(args.workload, args.n, world)
+    idx = list(range(len(w)))
     threads = os.cpu_count() or 1
-    sample = args.cpu_sample or 2048
-    rng = np.random.default_rng(1)
-    pick = sorted(rng.choice(len(idx), size=min(sample, len(idx)), replace=False).tolist())
-    geoms, ps, pgeo = layout(w, [idx[i] for i in pick])
+    # the K steps cover the batch once: step k takes every K-th direction from k
+    # (each slice has the batch's mix of geometries and dilations)
+    K = max(1, args.steps)
+    slices = [idx[k::K] for k in range(K)]
+    wg, wp, wpg = layout(w, idx[:64])
     for _ in range(args.warmup):
-        cpu_reference_run(geoms, ps[:64], pgeo[:64], threads)
-    times, nodes, pts, dirs = [], 0, 0, 0
-    for _ in range(args.steps):
+        cpu_reference_run(wg, wp, wpg, threads)
+    t_tot, nodes, pts, dirs = 0.0, 0, 0, 0
+    for sl in slices:
+        geoms, ps, pgeo = layout(w, sl)
         dt, nn, npt, nd = cpu_reference_run(geoms, ps, pgeo, threads)
-        times.append(dt)
-        nodes, pts, dirs = nn, npt, nd
-    t = float(np.mean(times))
-    v = nodes / t
+        t_tot += dt
+        nodes += nn
+        pts += npt
+        dirs += nd
+    t = t_tot / K
+    v = nodes / t_tot
     line = {"impl": "reference", "metric": metric, "value": v, "unit": "nodes/s", "n_gpus": 0,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int64",
-            "data": "synthetic (seeded)",
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int64+fp32",
+            "data": "synthetic (seeded CY instances, pfvs_b200/workloads.py)",
             "config": {"workload": workload_desc(args, w),
-                       "sample": f"{len(pick)} random directions (seed 1) of the batch per step",
+                       "steps_cover": f"the whole batch once: step k of {K} takes directions k, k+{K}, ...",
                        "threads": threads},
-            "directions_per_s": dirs / t, "points_per_s": pts / t,
+            "directions_per_s": dirs / t_tot, "points_per_s": pts / t_tot,
+            "reference_nodes": int(nodes), "directions_done": int(dirs), "points": int(pts),
             "cpu_baseline": {"value": v, "unit": "nodes/s", "cores": threads, "kind": "reference",
-                             "sample": f"{len(pick)} directions of the {args.workload} batch; "
-                                       f"the reference's own tree nodes"},
+                             "sample": f"all {len(idx)} directions of the {args.workload} batch once over the "
+                                       f"{K} steps; the reference kernel's own tree nodes (its float-pruned "
+                                       f"tree on its HNF basis)"},
             "e2e": {"value": v, "unit": "nodes/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
+
+
+def padded(ps_list):
+    """The p-vectors as one zero-padded 2-D array, the form the reference's coniZpM passes."""
+    ps = np.zeros((len(ps_list), max((len(p) for p in ps_list), default=1)), dtype=np.int64)
+    for i, p in enumerate(ps_list):
+        ps[i, :len(p)] = p
+    return ps
+
+
+def dataset_layout():
+    """The reference's own coni dataset geometries (tests/golden/dataset_pfvs.npz:
+    30 geometries, h11 3..9, 12,000 p-vectors), the workload on which the
+    post-processing produces PFVs."""
+    G = np.load(os.path.join(ROOT, "tests", "golden", "dataset_pfvs.npz"))
+    geoms, ps, pgeo = [], [], []
+    for k in range(int(G["n_geometries"][0])):
+        h, Q, m0 = (int(x) for x in G[f"g{k}_scal"])
+        geoms.append(dict(kappa=G[f"g{k}_kappa"], Mbasis=G[f"g{k}_Mbasis"], Q=Q,
+                          dilation=float(G[f"g{k}_D"][0]), M0min=m0))
+        for p in G[f"g{k}_ps"]:
+            ps.append(np.asarray(p, dtype=np.int64))
+            pgeo.append(k)
+    return geoms, ps, np.array(pgeo, dtype=np.int32)
+
+
+def pfv_rates(gpu, device, threads):
+    """PFVs/s on the dataset geometries: the device pipeline with its
+    post-processing (pfg_coni_pfvs) against the reference CPU kernel plus the
+    oracle's restatement of coniZpM's post-processing (pfvs/coni.py:275-412)."""
+    from oracle import postproc, ref
+    geoms, ps, pgeo = dataset_layout()
+    P = padded(ps)
+    gpu.coni_pfvs_multi(geoms, P, pgeo, device=device)                # warm
+    reps, dev_s, n_pfv = 5, 0.0, 0
+    for _ in range(reps):
+        K, M, pidx, pstat, secs, st = gpu.coni_pfvs_multi(geoms, P, pgeo, device=device)
+        dev_s += secs
+        n_pfv = len(pidx)
+    out = {"workload": f"{len(geoms)} reference dataset geometries (h11 3..9), {len(ps)} p-vectors",
+           "pfvs": int(n_pfv), "points": int(st["points"]), "device_ms": dev_s / reps * 1e3,
+           "pfvs_per_s": n_pfv * reps / dev_s if dev_s > 0 else None}
+    if ref.available():
+        t0 = time.perf_counter()
+        n_cpu = 0
+        lock = threading.Lock()
+
+        def one(k):
+            nonlocal n_cpu
+            g = geoms[k]
+            idx = np.flatnonzero(pgeo == k)
+            h = np.asarray(g["kappa"]).shape[0]
+            M_, Kn_, q_, pl, stt, _ = ref.coni_batch(g["kappa"], g["Mbasis"], np.array([ps[i] for i in idx]),
+                                                     g["Q"], g["dilation"], g["M0min"])
+            eK, eM, ek = postproc.pfvs_from_points(M_, Kn_, q_, pl, g["kappa"], h, g["Q"], g["M0min"])
+            with lock:
+                n_cpu += len(ek)
+        import concurrent.futures as cf
+        with cf.ThreadPoolExecutor(threads) as ex:
+            list(ex.map(one, range(len(geoms))))
+        dt = time.perf_counter() - t0
+        out["cpu_reference"] = {"pfvs": int(n_cpu), "seconds": dt, "pfvs_per_s": n_cpu / dt, "threads": threads,
+                                "what": "oracle/_ref kernel + the oracle's restated post-processing"}
+    return out
 
 
 def main():
@@ -270,89 +358,140 @@ def main():
     if args.impl == "reference":
         run_reference(args, world, rank, pg)
         return
-    from pfvs_b200 import build, gpu
+    from pfvs_b200 import build, gpu, multi
     build.build()
     if not gpu.available():
         raise SystemExit("bench: " + gpu.unavailable_reason())
     device = local
-    n_total = (args.n * world) if args.n else None
-    w, idx = workload_slice(args.workload, n_total, rank, world)
+    w = workload_for(args.workload, args.n, world)
+    idx = list(range(len(w)))
     geoms, ps_list, pgeo = layout(w, idx)
-    # the p-vectors as one zero-padded 2-D array, the form the reference's coniZpM passes
-    ps = np.zeros((len(ps_list), max((len(p) for p in ps_list), default=1)), dtype=np.int64)
-    for i, p in enumerate(ps_list):
-        ps[i, :len(p)] = p
+    ps = padded(ps_list)
     form = gpu.FORM_PLAIN if args.form == "plain" else gpu.FORM_BATCHED
     prec = {"auto": gpu.PREC_AUTO, "fp64": gpu.PREC_FP64, "fp32": gpu.PREC_FP32}[args.precision]
+    # one GPU: one call over the whole batch; several: contiguous chunks pulled
+    # by the ranks from a shared queue (the process group's store)
+    bounds = multi.chunk_bounds(len(ps), len(ps) if world == 1 else args.chunk)
+    store = pg.distributed_c10d._get_default_store() if pg is not None else None
+
+    def queue(key):
+        return multi.StoreQueue(store, "bench/" + key) if store is not None else multi.LocalQueue()
+
+    def call(k, **kw):
+        lo, hi = bounds[k]
+        return gpu.coni_batch_multi_ex(geoms, ps[lo:hi], pgeo[lo:hi], device=device, **kw)
 
     # work unit: nodes of the FP64-pruned tree with every GCD-cut row built (the
     # reference's pruning), counted once, untimed; the timed steps build the
-    # rows only where they pay off, which changes time but not the points
-    r64 = gpu.coni_batch_multi_ex(geoms, ps, pgeo, device=device, precision=gpu.PREC_FP64,
-                                  gcd_min_tree=-1.0)
-    nodes_fp64 = r64[6]["nodes"]
-    n_points = len(r64[2])
-    for _ in range(args.warmup):
-        r = gpu.coni_batch_multi_ex(geoms, ps, pgeo, device=device, form=form, precision=prec)
-    # parity guard: the timed form returns the FP64 form's arrays
-    for a, b in zip(r[:5], r64[:5]):
-        if not np.array_equal(a, b):
-            raise SystemExit("bench: timed form differs from the FP64 form")
+    # rows only where they pay off, which changes time but not the points.
+    # Parity guard: the timed form returns the FP64 form's arrays.
+    def unit(k):
+        r64 = call(k, precision=gpu.PREC_FP64, gcd_min_tree=-1.0)
+        r = call(k, form=form, precision=prec)
+        for a, b in zip(r[:5], r64[:5]):
+            if not np.array_equal(a, b):
+                raise SystemExit("bench: timed form differs from the FP64 form")
+        return r64[6]["nodes"], len(r64[2]), failed_by_status(r64[4]), len(r64[4])
+    got = multi.run_chunks(queue("unit"), len(bounds), unit)
+    nodes_fp64 = sum(g[0] for g in got.values())
+    n_points = sum(g[1] for g in got.values())
+    failed = {}
+    for g in got.values():
+        for k, v in g[2].items():
+            failed[k] = failed.get(k, 0) + v
+    for s_ in range(args.warmup):
+        multi.run_chunks(queue(f"warm{s_}"), len(bounds), lambda k: call(k, form=form, precision=prec)[5])
     # timed steps: device time (CUDA events inside the library)
+    tot = dict(ms_setup=0.0, ms_search=0.0, ms_output=0.0, nodes=0, launches=0)
+    failed_timed = {}
     barrier(pg)
     with Clocks(device) as clk:
-        dev_s, stats = 0.0, None
+        dev_s = 0.0
         t0 = time.perf_counter()
-        for _ in range(args.steps):
-            r = gpu.coni_batch_multi_ex(geoms, ps, pgeo, device=device, form=form, precision=prec)
-            dev_s += r[5]
-            stats = r[6]
+        for s_ in range(args.steps):
+            def timed(k):
+                r = call(k, form=form, precision=prec)
+                for key in tot:
+                    tot[key] += r[6][key]
+                for st_, v in failed_by_status(r[4]).items():
+                    failed_timed[st_] = failed_timed.get(st_, 0) + v
+                return r[5]
+            dev_s += sum(multi.run_chunks(queue(f"step{s_}"), len(bounds), timed).values())
         wall_s = time.perf_counter() - t0
     barrier(pg)
     dev_s = allmax(pg, dev_s)
     tot_nodes = allsum(pg, nodes_fp64)
     value = tot_nodes * args.steps / dev_s
-    # e2e: the public C ABI (pfg_coni_batch) with host buffers, wall clock
+    per_step = {k: v / args.steps for k, v in tot.items()}
+    # e2e: the public entry point (coni_batch_multi -> pfg_coni_batch) with host
+    # buffers (inputs copied in, rows copied out, every step), wall clock
     e2e = None
     if not args.no_e2e:
-        del r
-        out = gpu.coni_batch_multi(geoms, ps, pgeo, device=device)    # (warm-up: pinned output blocks)
-        del out
+        def e2e_call(k):
+            lo, hi = bounds[k]
+            out = gpu.coni_batch_multi(geoms, ps[lo:hi], pgeo[lo:hi], device=device)
+            return len(out[2]), hi - lo
+        multi.run_chunks(queue("e2e_warm"), len(bounds), e2e_call)   # (pinned output blocks)
         barrier(pg)
         t0 = time.perf_counter()
-        for _ in range(args.steps):
-            out = gpu.coni_batch_multi(geoms, ps, pgeo, device=device)
+        rows = dirs = 0
+        for s_ in range(args.steps):
+            for nr, nd in multi.run_chunks(queue(f"e2e{s_}"), len(bounds), e2e_call).values():
+                rows += nr
+                dirs += nd
         e2e_s = allmax(pg, time.perf_counter() - t0)
         MH = 64
-        h2d = len(ps) * MH * 8 + len(ps) * 4 + sum(np.asarray(g["kappa"]).size * 8 + np.asarray(g["Mbasis"]).size * 8
-                                                  for g in geoms) + len(geoms) * 32
-        d2h = len(out[2]) * (2 * MH * 8 + 16) + len(ps)
+        geo_bytes = sum(np.asarray(g["kappa"]).size * 8 + np.asarray(g["Mbasis"]).size * 8 for g in geoms) \
+            + len(geoms) * 32
+        h2d = dirs * (MH * 8 + 4) / args.steps + geo_bytes
+        d2h = rows * (2 * MH * 8 + 16) / args.steps + dirs / args.steps
         e2e = {"value": tot_nodes * args.steps / e2e_s, "unit": "nodes/s",
                "h2d_bytes_per_step": int(allsum(pg, h2d)), "d2h_bytes_per_step": int(allsum(pg, d2h)),
                "ms_per_step": e2e_s / args.steps * 1e3}
-    # CPU baseline: the reference kernel on a bounded sample (rank 0, N = 1)
+    threads = os.cpu_count() or 1
+    # CPU baseline: the reference kernel over the whole batch once (rank 0, N = 1)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         from oracle import ref
         if ref.available():
-            threads = os.cpu_count() or 1
-            sample = args.cpu_sample or 2048
-            rng = np.random.default_rng(1)
-            pick = sorted(rng.choice(len(idx), size=min(sample, len(idx)), replace=False).tolist())
-            g2, p2, pg2 = layout(w, [idx[i] for i in pick])
+            sel = idx if not args.cpu_sample else idx[::max(1, len(idx) // args.cpu_sample)]
+            g2, p2, pg2 = layout(w, sel)
             dt, rn, rp, rd = cpu_reference_run(g2, p2, pg2, threads)
             cpu = {"value": rn / dt, "unit": "nodes/s", "cores": threads, "kind": "reference",
-                   "sample": f"{len(pick)} random directions (seed 1) of the batch, "
-                             f"{dt:.1f} s on {threads} threads; the reference's own tree nodes",
-                   "directions_per_s": rd / dt}
-    # PFVs: the same batch through the device post-processing (pfg_coni_pfvs), once, untimed
+                   "sample": f"{len(sel)} of the batch's {len(idx)} directions, {dt:.1f} s on {threads} "
+                             f"threads; the reference kernel's own tree nodes ({rn})",
+                   "directions_per_s": rd / dt, "points_per_s": rp / dt}
+    # forms (N = 1): the plain form and the FP32-pruned form on the same work unit
+    forms = None
+    if rank == 0 and world == 1 and not args.no_extras:
+        forms = {}
+        for name, kw in (("plain", dict(form=gpu.FORM_PLAIN, precision=gpu.PREC_FP64)),
+                         ("fp32", dict(precision=gpu.PREC_FP32))):
+            call(0, **kw)
+            r = call(0, **kw)
+            if any(not np.array_equal(a, b) for a, b in zip(r[:4], call(0)[:4])):
+                raise SystemExit(f"bench: the {name} form's points differ")
+            forms[name] = {"ms_per_step": r[5] * 1e3, "search_ms": r[6]["ms_search"],
+                           "nodes_per_s": tot_nodes / r[5], "nodes_entered": r[6]["nodes"],
+                           "fp64_retries": r[6]["fp64_retries"]}
+        forms["batched_vs_plain"] = {"step": forms["plain"]["ms_per_step"] / (dev_s / args.steps * 1e3),
+                                     "search": forms["plain"]["search_ms"] / per_step["ms_search"]}
+        forms["batched_fp32_vs_plain"] = {"step": forms["plain"]["ms_per_step"] / forms["fp32"]["ms_per_step"],
+                                          "search": forms["plain"]["search_ms"] / forms["fp32"]["search_ms"]}
+    # PFVs: the batch through the device post-processing (pfg_coni_pfvs), once,
+    # untimed, and PFVs/s on the reference's dataset geometries (which have PFVs)
     pfv = None
-    if not args.no_e2e:
-        Kp, Mp, pp, sp, secs_p, st_p = gpu.coni_pfvs_multi(geoms, ps, pgeo, device=device)
-        pfv = {"pfvs_per_step": int(allsum(pg, len(pp))), "points_in": int(allsum(pg, st_p["points"])),
-               "device_ms": allmax(pg, secs_p) * 1e3,
-               "pfvs_per_s": allsum(pg, len(pp)) / max(allmax(pg, secs_p), 1e-12)}
-        del Kp, Mp, pp
+    if not args.no_extras:
+        def pfv_chunk(k):
+            lo, hi = bounds[k]
+            Kp, Mp, pp, sp, secs_p, st_p = gpu.coni_pfvs_multi(geoms, ps[lo:hi], pgeo[lo:hi], device=device)
+            return len(pp), st_p["points"], secs_p
+        pr = multi.run_chunks(queue("pfv"), len(bounds), pfv_chunk).values()
+        pfv = {"pfvs_per_step": int(allsum(pg, sum(x[0] for x in pr))),
+               "points_in": int(allsum(pg, sum(x[1] for x in pr))),
+               "device_ms": allmax(pg, sum(x[2] for x in pr)) * 1e3}
+        if rank == 0 and world == 1:
+            pfv["dataset"] = pfv_rates(gpu, device, threads)
     # roofline of the search kernel: executed warp instructions per launch (ncu
     # per-node figure x the launch's nodes) over its CUDA-event time (the
     # search stage: k_flip, a few microseconds, then k_search<double, 1>); the
@@ -361,21 +500,24 @@ def main():
     clk_sum = clk.summary()
     mhz = clk_sum.get("sm_mhz") or peaks.get("sm_max_mhz", 1965.0)
     peak = N_SM * SCHEDULERS * mhz * 1e6
-    search_s = stats["ms_search"] / 1e3
-    achieved = SEARCH_INST_PER_NODE * stats["nodes"] / search_s
+    search_s = per_step["ms_search"] / 1e3
+    achieved = SEARCH_INST_PER_NODE * per_step["nodes"] / search_s
     roofline = {"kernel": "k_search<double, 1>", "bound": "issue", "achieved": achieved, "peak": peak,
                 "unit": "warp-inst/s", "frac": achieved / peak,
-                "traffic": SEARCH_DRAM_PER_NODE * stats["nodes"],
+                "traffic": SEARCH_DRAM_PER_NODE * per_step["nodes"],
                 "basis": f"ncu: {SEARCH_INST_PER_NODE:.0f} warp-inst and {SEARCH_DRAM_PER_NODE:.1f} DRAM bytes per "
-                         f"search node x {stats['nodes']} nodes per launch; peak = {N_SM} SMs x {SCHEDULERS} x "
+                         f"search node x {per_step['nodes']:.0f} nodes per step; peak = {N_SM} SMs x {SCHEDULERS} x "
                          f"{mhz:.0f} MHz (sampled SM clock); HBM for context: {peaks.get('hbm_gbs')} GB/s {peaks_kind}"}
-    setup_s = stats["ms_setup"] / 1e3
-    setup_ach = SETUP_INST_PER_DIR * len(idx) / setup_s
+    setup_s = per_step["ms_setup"] / 1e3
+    n_here = len(idx) / world
+    setup_ach = SETUP_INST_PER_DIR * n_here / setup_s
     roofline_setup = {"kernel": "k_setup<32, 0..2>", "bound": "issue", "achieved": setup_ach, "peak": peak,
                       "unit": "warp-inst/s", "frac": setup_ach / peak,
-                      "traffic": SETUP_DRAM_PER_DIR * len(idx),
+                      "traffic": SETUP_DRAM_PER_DIR * n_here,
                       "basis": f"ncu: {SETUP_INST_PER_DIR:.0f} warp-inst and {SETUP_DRAM_PER_DIR:.0f} DRAM bytes "
-                               f"per direction over the three phases x {len(idx)} directions"}
+                               f"per direction over the three phases x {n_here:.0f} directions"}
+    failed_all = {str(k): int(allsum(pg, v)) for k, v in sorted(failed.items())}
+    failed_step = {str(k): allsum(pg, v) / args.steps for k, v in sorted(failed_timed.items())}
     if rank == 0:
         line = {"metric": "lattice nodes/s", "value": value, "unit": "nodes/s", "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup,
@@ -385,16 +527,20 @@ def main():
                 "data": "synthetic (seeded CY instances, pfvs_b200/workloads.py)",
                 "config": {"workload": workload_desc(args, w),
                            "form": args.form, "precision": args.precision,
-                           "directions_per_gpu": len(idx),
+                           "directions_per_gpu": len(idx) // world,
                            "l2": "working set per step > 126 MB (slabs + points); no flush needed",
-                           "parallelism": f"directions sharded over {world} GPU(s)"},
+                           "parallelism": (f"directions in chunks of {bounds[0][1]} pulled by {world} GPUs "
+                                           f"from a shared queue" if world > 1 else "one GPU, one call")},
                 "nodes_fp64_per_step": int(tot_nodes), "points_per_step": int(allsum(pg, n_points)),
-                "directions_per_s": allsum(pg, len(idx)) * args.steps / dev_s,
-                "stage_ms": {"setup": stats["ms_setup"], "search": stats["ms_search"],
-                             "output": stats["ms_output"]},
-                "timed_form_nodes_per_step": stats["nodes"], "wall_ms_per_step": wall_s / args.steps * 1e3,
-                "clocks": clk_sum, "e2e": e2e, "cpu_baseline": cpu, "roofline": roofline, "roofline_setup": roofline_setup, "pfvs": pfv,
-                "gpu_launches": int(stats.get("launches", 0)) * args.steps}
+                "directions_per_s": len(idx) * args.steps / dev_s,
+                "points_per_s": allsum(pg, n_points) * args.steps / dev_s,
+                "failed_directions": failed_all, "failed_directions_timed_per_step": failed_step,
+                "stage_ms": {"setup": per_step["ms_setup"], "search": per_step["ms_search"],
+                             "output": per_step["ms_output"]},
+                "timed_form_nodes_per_step": int(per_step["nodes"]), "wall_ms_per_step": wall_s / args.steps * 1e3,
+                "clocks": clk_sum, "e2e": e2e, "cpu_baseline": cpu, "roofline": roofline,
+                "roofline_setup": roofline_setup, "forms": forms, "pfvs": pfv,
+                "gpu_launches": int(tot["launches"])}
         print(json.dumps(line))
     if pg is not None:
         pg.destroy_process_group()
