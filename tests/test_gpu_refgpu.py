@@ -1,0 +1,68 @@
+"""
+GPU: this library against the reference's own CUDA backend
+(pfvs/fp_kernel/cuda/pfvs_gpu.cu, built unmodified for sm_100a by
+`make -C oracle refgpu`, run in a subprocess of its own through the same C
+ABI).  That backend compiles only up to h11 = 24 (PFL_MAX_H11), so the cases
+are configurations 1 and 2 (its default build, PFL_MAX_H11 = 12) and the
+h11 in {8, 16, 24} part of configuration 3 (the 24 build).  Its pstat 1
+marks directions it hands to the reference's CPU path; on the others the
+(M, Kn, q, pidx) arrays must be identical, element for element, as the
+reference's tests/test_gpu.py:60-63 compares its GPU and CPU arrays.
+"""
+import numpy as np
+import pytest
+
+from oracle import refgpu
+from pfvs_b200 import gpu, workloads
+from parity import assert_same, layout
+
+pytestmark = pytest.mark.gpu
+
+# (workload, directions, dilations, seed, h11 limit of the build, min points)
+CASES = [
+    ("small", None, None, 0, 12, 0),           # config 1
+    ("small", 256, (300.0,), 4, 12, 10),
+    ("plain", None, None, 0, 12, 0),           # config 2
+    ("plain", 4096, (300.0,), 0, 12, 100),
+    ("mixed", None, None, 0, 24, 1_000_000),   # config 3, its h11 <= 24 directions
+]
+
+
+@pytest.fixture(scope="module", autouse=True)
+def _built(lib):
+    if not gpu.available():
+        pytest.fail("no CUDA device: " + gpu.unavailable_reason())
+    if not (refgpu.available(12) and refgpu.available(24)):
+        pytest.skip("the reference CUDA backend is not built (make -C oracle refgpu)")
+
+
+def _id(c):
+    return f"{c[0]}-{c[1] or 'cfg'}-dil{'x'.join(str(int(x)) for x in c[2]) if c[2] else 'cfg'}-s{c[3]}"
+
+
+def _restrict(geoms, ps, pgeo, hs, hmax):
+    """The directions of geometries with h11 <= hmax, re-indexed."""
+    keep_g = [k for k, h in enumerate(hs) if h <= hmax]
+    remap = {k: i for i, k in enumerate(keep_g)}
+    sel = [i for i in range(len(ps)) if pgeo[i] in remap]
+    return ([geoms[k] for k in keep_g], [ps[i] for i in sel],
+            np.array([remap[pgeo[i]] for i in sel], dtype=np.int32))
+
+
+@pytest.mark.parametrize("case", CASES, ids=[_id(c) for c in CASES])
+def test_matches_reference_cuda_backend(case, record_property):
+    name, n, dils, seed, hmax, min_points = case
+    w = workloads.build(name, n_p=n, dilations=dils, seed=seed)
+    geoms, ps, pgeo, hs = layout(w)
+    geoms, ps, pgeo = _restrict(geoms, ps, pgeo, hs, hmax)
+    got = gpu.coni_batch_multi(geoms, ps, pgeo)
+    assert np.all(got[4] == 0)
+    ref = refgpu.coni_batch_multi(geoms, ps, pgeo, max_h11=hmax)
+    done = ref[4] == 0
+    record_property("directions", len(ps))
+    record_property("reference_gpu_finished", float(done.mean()))
+    print(f"{_id(case)}: {len(ps)} directions, reference CUDA backend finished {done.mean():.4f}, "
+          f"{len(ref[2])} points")
+    assert done.mean() >= 0.9
+    assert_same(got, ref, ok_mask=done)
+    assert int(np.sum(done[got[3]])) >= min_points
