@@ -15,7 +15,11 @@
  *       -9  the ellipsoid matrix is not positive definite
  *       -20 an exact setup value exceeds the device's fixed-width integers
  *       -21 the FP64 factor could not be certified (ill-conditioned)
+ *       -22 a direction's search ran past its deadline (pfg_options.deadline_s)
  *   - pfg_max_h11() is 64.
+ *   - Out of device memory (a shared or partly filled GPU), a call frees its
+ *     per-batch buffers, halves the batch and carries on from the batch it
+ *     was on, as the reference's backend does (pfvs_gpu.cu:729-747).
  *
  * The remaining entry points are extensions of this library.
  */
@@ -92,6 +96,19 @@ typedef struct {
                                   search tree has at least this many nodes (they only
                                   prune; results are identical either way).  0: the
                                   library default; < 0: always (the reference's pruning) */
+    double wait_s;             /* bound on a search warp's wait for work, counted from the
+                                  launch: past it the call fails (rc 1, "a bounded device
+                                  wait ran out").  0: 30 s */
+    double deadline_s;         /* bound on one subtree's search: past it the direction gets
+                                  status -22 and the call goes on.  0: 120 s */
+    int check_fp32;            /* with PFG_PREC_FP32: run the FP32 pass with an FP64 shadow of
+                                  its pruning bounds (one warp per direction, no work
+                                  sharing; same points) and report the bound errors in
+                                  pfg_stats.fp32_* (a measurement mode, slower) */
+    int compact_rows;          /* pfg_coni_batch_ex only: M and Kn rows w entries wide, w the
+                                  largest h11 of in->h, instead of pfg_max_h11() (fewer bytes to
+                                  copy back when every h11 is small; pfg_coni_batch keeps the
+                                  reference's layout) */
 } pfg_options;
 
 /* Statistics of one call. */
@@ -104,6 +121,13 @@ typedef struct {
     int64_t fp64_retries;      /* directions re-searched in FP64 after -11 */
     double  ms_setup, ms_search, ms_output;   /* device time per stage */
     int64_t launches;          /* kernels this library launched */
+    int64_t batch_retries;     /* batches redone at half size after a device allocation failed */
+    /* with pfg_options.check_fp32: the FP32 pruning bounds against FP64 (the FP64 values
+     * standing in for the exact ones), maxima over every node and candidate of the FP32 pass */
+    double  fp32_rem_err;      /* |remaining norm (FP32) - (FP64)|, in units of q */
+    double  fp32_margin_frac;  /* that error over the FP32 test's safety margin (slack + en) */
+    double  fp32_end_err;      /* |interval endpoint (FP32) - (FP64)|, in coordinate units */
+    int64_t fp32_narrower;     /* levels whose FP32 integer range misses part of the FP64 one */
 } pfg_stats;
 
 /* pfg_coni_batch with options and statistics (opt, stats may be NULL);
@@ -137,25 +161,37 @@ int pfg_coni_pfvs(const pfg_input *in, const pfg_options *opt, pfg_pfv_output *o
 /* Free a pfg_pfv_output's arrays (safe on a zeroed struct). */
 void pfg_pfv_output_free(pfg_pfv_output *out);
 
+/* Test hook (no counterpart in the reference): the k-th device allocation
+ * this library makes from now on (k >= 1) fails once with
+ * cudaErrorMemoryAllocation, without allocating, so that tests can drive the
+ * out-of-memory path of the batch loop; k <= 0 cancels. */
+void pfg_debug_fail_alloc(int k);
+
 /*
  * No counterpart in the reference.  The coni pipeline for ONE p-vector,
- * for callers that cannot allocate device memory while they run (code in a
- * framework that owns all device memory through its own pool or arena, such
- * as an XLA custom call or a TensorRT plugin; work issued while a stream is
- * being captured; a real-time path that may not block on the allocator).
- * The call allocates nothing: no cudaMalloc/cudaFree, no host allocation.
+ * for callers that cannot allocate device memory while they run: code in a
+ * framework that owns all device memory through its own pool or arena (an
+ * XLA custom call, a TensorRT plugin, an inference server with a fixed
+ * memory budget), where a cudaMalloc would go around that pool or fail
+ * because the pool holds the memory; or a real-time path that may not block
+ * on the allocator.  The call allocates nothing: no cudaMalloc/cudaFree, no
+ * host allocation.
  *
  * Inputs (device pointers): kappa (h^3), Mbasis (h^2, basis vectors as
  * columns), p (h entries, p[0] = 0); scalars h (3..64), Q, qmax =
  * floor(dilation Q), linmin = ceil(M0min).  Outputs (device pointers, the
  * caller's): M and Kn (cap x 64 int64, rows as pfg_output's), q (cap),
- * n_out (1 int64: the number of rows) and status (1 int32: 0 done, -2 more
- * than cap or PFG_STATIC_MAX_POINTS points, else a status of pfg_output's
- * pstat).  The rows are exactly pfg_coni_batch's rows for that p-vector, in
- * the same order.  The work is queued on `stream` (a cudaStream_t, or NULL);
- * the outputs are valid once it completes.  Returns 0 when queued, 1 on bad
- * arguments (message on stderr): h outside 3..64, cap outside
- * 0..PFG_STATIC_MAX_POINTS.
+ * n_out (1 int64: the number of rows) and status (1 int32):
+ *    0  done
+ *   -2  more than cap or PFG_STATIC_MAX_POINTS points (n_out is then 0)
+ *   -22 the search ran past its 120 s deadline
+ *   else a status of pfg_output's pstat (-8, -9, -20, -21).
+ * The rows are exactly pfg_coni_batch's rows for that p-vector, in the same
+ * order.  The whole call runs on ONE warp (no work sharing), so a direction
+ * with a large search tree takes far longer than in pfg_coni_batch.  The work
+ * is queued on `stream` (a cudaStream_t, or NULL); the outputs are valid once
+ * it completes.  Returns 0 when queued, 1 on bad arguments (message on
+ * stderr): h outside 3..64, cap outside 0..PFG_STATIC_MAX_POINTS.
  *
  * The scratch (about 3 MB) is a static device array that every GPU loading
  * this library holds until the process exits.  All calls share it: calls
@@ -163,7 +199,10 @@ void pfg_pfv_output_free(pfg_pfv_output *out);
  * them one after another.  Each call clears what must start at zero; the
  * array otherwise keeps the last call's contents.  The first call on a
  * device looks up the array's device address (cudaGetSymbolAddress) with
- * that device current; make that first call before any stream capture.
+ * that device current and keeps it for the process; make that first call
+ * before any stream capture.  After cudaDeviceReset the kept address is
+ * stale: do not call this entry point in a process that has reset a device
+ * it used.
  */
 #define PFG_STATIC_MAX_POINTS 2048
 int pfg_coni_direction_static(int h, int64_t Q, int64_t qmax, int64_t linmin,

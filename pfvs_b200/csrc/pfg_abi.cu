@@ -15,6 +15,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cstdarg>
 #include <cstdio>
@@ -84,6 +85,9 @@ Workspace &workspace(int dev)
     return *w;
 }
 
+// pfg_debug_fail_alloc: allocations left before the one made to fail (0: none)
+std::atomic<int> g_fail_alloc{0};
+
 cudaError_t ws_get(Workspace &W, int slot, size_t bytes, void **out)
 {
     if (bytes == 0) bytes = 16;
@@ -92,6 +96,7 @@ cudaError_t ws_get(Workspace &W, int slot, size_t bytes, void **out)
         W.p[slot] = nullptr;
         W.cap[slot] = 0;
         size_t b = bytes + bytes / 8 + 256;
+        if (g_fail_alloc.load() > 0 && g_fail_alloc.fetch_sub(1) == 1) return cudaErrorMemoryAllocation;
         cudaError_t e = cudaMalloc(&W.p[slot], b);
         if (e != cudaSuccess) { W.p[slot] = nullptr; return e; }
         W.cap[slot] = b;
@@ -100,9 +105,9 @@ cudaError_t ws_get(Workspace &W, int slot, size_t bytes, void **out)
     return cudaSuccess;
 }
 
-void ws_release(Workspace &W)
+void ws_release(Workspace &W, int keep_below = 0)
 {
-    for (int k = 0; k < W_N; ++k) {
+    for (int k = keep_below; k < W_N; ++k) {
         if (W.p[k]) cudaFree(W.p[k]);
         W.p[k] = nullptr;
         W.cap[k] = 0;
@@ -190,10 +195,12 @@ void pinned_release_idle()
 struct RowSink {
     int64_t *M = nullptr, *Kn = nullptr, *q = nullptr, *pidx = nullptr;
     size_t n = 0, cap = 0;
-    bool alloc(size_t rows)
+    int w = MH;                                 // entries per M / Kn row
+    bool alloc(size_t rows, int width)
     {
-        M = (int64_t *)pinned_get(rows * MH * 8);
-        Kn = (int64_t *)pinned_get(rows * MH * 8);
+        w = width;
+        M = (int64_t *)pinned_get(rows * w * 8);
+        Kn = (int64_t *)pinned_get(rows * w * 8);
         q = (int64_t *)pinned_get(rows * 8);
         pidx = (int64_t *)pinned_get(rows * 8);
         cap = rows;
@@ -249,6 +256,13 @@ const std::vector<uint32_t> &primes31()
     return P;
 }
 
+double dbits(unsigned long long b)
+{
+    double x;
+    memcpy(&x, &b, sizeof x);
+    return x;
+}
+
 void set_err(pfg_output *out, const char *fmt, ...)
 {
     va_list ap;
@@ -262,6 +276,9 @@ void set_err(pfg_output *out, const char *fmt, ...)
 #define CK(x) do { cudaError_t e_ = (x); if (e_ != cudaSuccess) { \
     set_err(out, "%s (%s:%d)", cudaGetErrorString(e_), __FILE__, __LINE__); rc = 1; goto fail; } } while (0)
 #define WS(ptr, slot, bytes) CK(ws_get(W, slot, (size_t)(bytes), (void **)&(ptr)))
+// inside the batch loop: out of device memory -> the batch again at half size
+#define WSB(ptr, slot, bytes) do { cudaError_t eb_ = ws_get(W, slot, (size_t)(bytes), (void **)&(ptr)); \
+    if (eb_ == cudaErrorMemoryAllocation && nb > 1) goto out_of_memory; CK(eb_); } while (0)
 
 extern "C" int pfg_max_h11(void) { return MH; }
 
@@ -308,6 +325,8 @@ extern "C" void pfg_release(int device)
     pinned_release_idle();
 }
 
+extern "C" void pfg_debug_fail_alloc(int k) { g_fail_alloc.store(k > 0 ? k : 0); }
+
 extern "C" int pfg_coni_batch(const pfg_input *in, pfg_output *out)
 {
     return pfg_coni_batch_ex(in, nullptr, out, nullptr, nullptr);
@@ -320,12 +339,22 @@ static int coni_run(const pfg_input *in, const pfg_options *opt_in, pfg_output *
 {
     memset(out, 0, sizeof *out);
     if (stats) memset(stats, 0, sizeof *stats);
-    pfg_options opt = {PFG_FORM_BATCHED, PFG_PREC_AUTO, 0, 0, 0.0};
+    pfg_options opt = {PFG_FORM_BATCHED, PFG_PREC_AUTO, 0, 0, 0.0, 0.0, 0.0, 0, 0};
     if (opt_in) opt = *opt_in;
+    const long long wait_ns = opt.wait_s > 0 ? (long long)(opt.wait_s * 1e9) : 30ll * 1000000000ll;
+    const long long deadline_ns = opt.deadline_s > 0 ? (long long)(opt.deadline_s * 1e9) : 120ll * 1000000000ll;
     const double gcd_min_tree = opt.gcd_min_tree == 0.0 ? GCD_MIN_TREE_DEFAULT
                                 : (opt.gcd_min_tree < 0.0 ? 0.0 : opt.gcd_min_tree);
     const int64_t NP = in->n_p;
     if (NP < 0 || in->n_geo < 0) { set_err(out, "negative sizes"); return 1; }
+    // width of the M / Kn rows handed back: MH (the reference's layout), or with
+    // compact_rows the widest h11 of the call (the PFV path keeps MH internally)
+    int rw = MH;
+    if (opt.compact_rows && !pfv) {
+        rw = 3;
+        for (int gi = 0; gi < in->n_geo; ++gi) rw = std::max(rw, (int)in->h[gi]);
+        rw = std::min(rw, MH);
+    }
     std::vector<Geo> geos(in->n_geo);
     {
         int64_t koff = 0, moff = 0;
@@ -403,7 +432,9 @@ static int coni_run(const pfg_input *in, const pfg_options *opt_in, pfg_output *
         }
         unsigned long long &pts_cap = W.pts_cap;
         const unsigned q_cap = 1u << 20;
-        for (int64_t off = 0; off < NP;) {
+        int64_t off = 0;
+    next_batches:
+        for (; off < NP;) {
             const int nb = (int)std::min<int64_t>(batch, NP - off);
             int64_t *dps; int32_t *dpgeo; int64_t *dslaboff, *dslab; Dir *ddirs; SetupScratch *dscr;
             int32_t *dtodo32, *dtodoall, *dorder; SearchCtl *dctl; WorkItem *ditems; int *dready;
@@ -450,21 +481,21 @@ static int coni_run(const pfg_input *in, const pfg_options *opt_in, pfg_output *
                 }
             }
             const int setup_warps = std::max(grid32, 4 * std::max(grid64[0], std::max(grid64[1], grid64[2])));
-            WS(dps, W_PS, (size_t)nb * MH * 8);
-            WS(dpgeo, W_PGEO, (size_t)nb * 4);
-            WS(dslaboff, W_SLABOFF, (size_t)nb * 8);
-            WS(dslab, W_SLAB, (size_t)slab_total * 8);
-            WS(ddirs, W_DIRS, (size_t)nb * sizeof(Dir));
-            WS(dscr, W_SCRATCH, (size_t)setup_warps * sizeof(SetupScratch));
-            WS(dtodo32, W_TODO32, (size_t)std::max<size_t>(todo32.size(), 1) * 4);
-            WS(dtodoall, W_TODOALL, (size_t)nb * 4);
-            WS(dorder, W_ORDER, (size_t)nb * 4);
-            WS(dctl, W_CTL, 2 * sizeof(SearchCtl) + 64);
-            WS(ditems, W_ITEMS, (size_t)q_cap * sizeof(WorkItem));
-            WS(dready, W_READY, (size_t)q_cap * 4);
-            WS(ddirnodes, W_DIRNODES, (size_t)nb * 8);
-            WS(ddirpass, W_DIRPASS, (size_t)nb * 4);
-            WS(dretry, W_RETRY, 64);
+            WSB(dps, W_PS, (size_t)nb * MH * 8);
+            WSB(dpgeo, W_PGEO, (size_t)nb * 4);
+            WSB(dslaboff, W_SLABOFF, (size_t)nb * 8);
+            WSB(dslab, W_SLAB, (size_t)slab_total * 8);
+            WSB(ddirs, W_DIRS, (size_t)nb * sizeof(Dir));
+            WSB(dscr, W_SCRATCH, (size_t)setup_warps * sizeof(SetupScratch));
+            WSB(dtodo32, W_TODO32, (size_t)std::max<size_t>(todo32.size(), 1) * 4);
+            WSB(dtodoall, W_TODOALL, (size_t)nb * 4);
+            WSB(dorder, W_ORDER, (size_t)nb * 4);
+            WSB(dctl, W_CTL, 2 * sizeof(SearchCtl) + 64);
+            WSB(ditems, W_ITEMS, (size_t)q_cap * sizeof(WorkItem));
+            WSB(dready, W_READY, (size_t)q_cap * 4);
+            WSB(ddirnodes, W_DIRNODES, (size_t)nb * 8);
+            WSB(ddirpass, W_DIRPASS, (size_t)nb * 4);
+            WSB(dretry, W_RETRY, 64);
             CK(cudaMemcpy(dps, &in->ps[off * MH], (size_t)nb * MH * 8, cudaMemcpyHostToDevice));
             CK(cudaMemcpy(dpgeo, &in->pgeo[off], (size_t)nb * 4, cudaMemcpyHostToDevice));
             CK(cudaMemcpy(dslaboff, slab_off.data(), (size_t)nb * 8, cudaMemcpyHostToDevice));
@@ -474,8 +505,8 @@ static int coni_run(const pfg_input *in, const pfg_options *opt_in, pfg_output *
             CK(cudaMemcpy(dorder, order.data(), (size_t)nb * 4, cudaMemcpyHostToDevice));
 
         restart_search:
-            WS(dhdr, W_HDR, pts_cap * sizeof(PointHdr));
-            WS(dcoords, W_COORDS, pts_cap * MD * 4);
+            WSB(dhdr, W_HDR, pts_cap * sizeof(PointHdr));
+            WSB(dcoords, W_COORDS, pts_cap * MD * 4);
             CK(cudaMemset(dctl, 0, 2 * sizeof(SearchCtl) + 64));
             CK(cudaMemset(ddirnodes, 0, (size_t)nb * 8));
             CK(cudaMemset(dretry, 0, 64));
@@ -506,9 +537,9 @@ static int coni_run(const pfg_input *in, const pfg_options *opt_in, pfg_output *
                 SearchArgs A{};
                 A.geo = dgeo; A.dirs = ddirs; A.slab = dslab; A.pass = 1; A.items = ditems;
                 A.ready = dready; A.q_cap = q_cap; A.hdr = dhdr; A.coords = dcoords; A.pts_cap = pts_cap;
-                A.dir_nodes = ddirnodes; A.eps = 1e-4; A.wait_ns = 30ll * 1000000000ll;
+                A.dir_nodes = ddirnodes; A.eps = 1e-4; A.wait_ns = wait_ns;
                 A.npts = &dctl->npts;
-                A.deadline_ns = 120ll * 1000000000ll;
+                A.deadline_ns = deadline_ns;
                 // per-warp staging area in shared memory, sized for the batch's largest h11
                 int hmax = 3;
                 for (int k = 0; k < nb; ++k) hmax = std::max(hmax, geos[in->pgeo[off + k]].h);
@@ -524,6 +555,7 @@ static int coni_run(const pfg_input *in, const pfg_options *opt_in, pfg_output *
                 void (*ks32)(SearchArgs) = one ? k_search<float, 1> : k_search<float, 2>;
                 void (*ks64)(SearchArgs) = one ? k_search<double, 1> : k_search<double, 2>;
                 void (*kplain)(SearchArgs, int) = one ? k_search_plain<double, 1> : k_search_plain<double, 2>;
+                void (*kchk32)(SearchArgs, int) = one ? k_search_plain<float, 1, true> : k_search_plain<float, 2, true>;
                 CK(cudaFuncSetAttribute((const void *)ks32, cudaFuncAttributeMaxDynamicSharedMemorySize, wpb32 * st32));
                 CK(cudaFuncSetAttribute((const void *)ks64, cudaFuncAttributeMaxDynamicSharedMemorySize, wpb64 * st64));
                 if (opt.form == PFG_FORM_PLAIN) {
@@ -548,7 +580,15 @@ static int coni_run(const pfg_input *in, const pfg_options *opt_in, pfg_output *
                     };
                     A.donate = 1;
                     // FP32 pass over the FP32 geometries' directions
-                    if (!todo32.empty()) {
+                    if (!todo32.empty() && opt.check_fp32) {
+                        // the bound-check form: one warp per direction with the FP64 shadow
+                        CK(cudaFuncSetAttribute((const void *)kchk32, cudaFuncAttributeMaxDynamicSharedMemorySize, st32));
+                        SearchArgs C = A;
+                        C.donate = 0; C.n_warps = 1; C.stage_bytes = st32; C.ctl = dctl;
+                        C.todo = dtodo32; C.n_todo = (int)todo32.size(); C.pass = 1;
+                        kchk32<<<(int)todo32.size(), 32, st32>>>(C, -1); ++launches;
+                        CK(cudaGetLastError());
+                    } else if (!todo32.empty()) {
                         int grid = 0;
                         CK(grid_for((const void *)ks32, wpb32, st32, grid));
                         A.n_warps = grid * wpb32; A.stage_bytes = st32;
@@ -594,18 +634,18 @@ static int coni_run(const pfg_input *in, const pfg_options *opt_in, pfg_output *
             unsigned *dcount, *dfill, *didx, *dperm, *dperm2, *dsidx;
             unsigned long long *dseg, *dcseg, *dsum; int64_t *dkeys;
             const unsigned long long np1 = std::max<unsigned long long>(npts, 1);
-            WS(dcount, W_COUNT, (size_t)nb * 4);
-            WS(dfill, W_FILL, (size_t)nb * 4);
-            WS(dseg, W_SEG, (size_t)(nb + 1) * 8);
-            WS(dcseg, W_CSEG, (size_t)(nb + 1) * 8);
-            WS(dsum, W_SUM, 64);
-            WS(didx, W_IDX, np1 * 4);
-            WS(dperm, W_PERM, np1 * 4);
-            WS(dperm2, W_PERM2, np1 * 4);
-            WS(dsidx, W_SIDX, np1 * 4);
+            WSB(dcount, W_COUNT, (size_t)nb * 4);
+            WSB(dfill, W_FILL, (size_t)nb * 4);
+            WSB(dseg, W_SEG, (size_t)(nb + 1) * 8);
+            WSB(dcseg, W_CSEG, (size_t)(nb + 1) * 8);
+            WSB(dsum, W_SUM, 64);
+            WSB(didx, W_IDX, np1 * 4);
+            WSB(dperm, W_PERM, np1 * 4);
+            WSB(dperm2, W_PERM2, np1 * 4);
+            WSB(dsidx, W_SIDX, np1 * 4);
             int ks = 3;
             for (int k = 0; k < nb; ++k) ks = std::max(ks, geos[in->pgeo[off + k]].h);
-            WS(dkeys, W_KEYS, np1 * ks * 8);
+            WSB(dkeys, W_KEYS, np1 * ks * 8);
             CK(cudaMemset(dcount, 0, (size_t)nb * 4));
             CK(cudaMemset(dfill, 0, (size_t)nb * 4));
             CK(cudaEventRecord(ev[3]));
@@ -625,10 +665,10 @@ static int coni_run(const pfg_input *in, const pfg_options *opt_in, pfg_output *
                 W.copy_pending[slot] = false;
             }
             int64_t *oM, *oK, *oq, *op;
-            WS(oM, slot ? W_OM2 : W_OM, std::max<unsigned long long>(n_out, 1) * MH * 8);
-            WS(oK, slot ? W_OK2 : W_OK, std::max<unsigned long long>(n_out, 1) * MH * 8);
-            WS(oq, slot ? W_OQ2 : W_OQ, std::max<unsigned long long>(n_out, 1) * 8);
-            WS(op, slot ? W_OP2 : W_OP, std::max<unsigned long long>(n_out, 1) * 8);
+            WSB(oM, slot ? W_OM2 : W_OM, std::max<unsigned long long>(n_out, 1) * rw * 8);
+            WSB(oK, slot ? W_OK2 : W_OK, std::max<unsigned long long>(n_out, 1) * rw * 8);
+            WSB(oq, slot ? W_OQ2 : W_OQ, std::max<unsigned long long>(n_out, 1) * 8);
+            WSB(op, slot ? W_OP2 : W_OP, std::max<unsigned long long>(n_out, 1) * 8);
             if (n_out) {
                 const int smem_sort = SORT_CAP * KEYN * 8 + SORT_CAP * 4;
                 CK(cudaFuncSetAttribute(k_segsort, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_sort));
@@ -641,7 +681,7 @@ static int coni_run(const pfg_input *in, const pfg_options *opt_in, pfg_output *
                     std::swap(pin, pout);
                 }
                 k_order<<<nsm * 4, 256>>>(O, n_out, pin, dsidx, pout); ++launches;
-                RowArgs R{ddirs, dslab, dhdr, dcoords, dsidx, pout, dkeys, ks, n_out, off, oM, oK, oq, op};
+                RowArgs R{ddirs, dslab, dhdr, dcoords, dsidx, pout, dkeys, ks, n_out, off, oM, oK, oq, op, rw};
                 k_rows<<<nsm * 8, 256>>>(R); ++launches;
                 CK(cudaGetLastError());
             }
@@ -650,11 +690,11 @@ static int coni_run(const pfg_input *in, const pfg_options *opt_in, pfg_output *
                 pfv->n_points += (int64_t)n_out;
                 unsigned long long *pcnt, *pkeep; uint64_t *pkg; unsigned *pept, *peord, *psort;
                 int64_t *peg, *pek0; int *pnons, *perr; uint32_t *dprimes;
-                WS(pcnt, W_PCNT, (n_out + 1) * 8);
-                WS(pkg, W_PKG, n_out * 8);
-                WS(pnons, W_PNONS, n_out * 4);
-                WS(perr, W_PERR, 64);
-                WS(dprimes, W_PRIMES, primes31().size() * 4);
+                WSB(pcnt, W_PCNT, (n_out + 1) * 8);
+                WSB(pkg, W_PKG, n_out * 8);
+                WSB(pnons, W_PNONS, n_out * 4);
+                WSB(perr, W_PERR, 64);
+                WSB(dprimes, W_PRIMES, primes31().size() * 4);
                 CK(cudaMemset(perr, 0, 64));
                 CK(cudaMemcpy(dprimes, primes31().data(), primes31().size() * 4, cudaMemcpyHostToDevice));
                 int hmax2 = 3;
@@ -669,12 +709,12 @@ static int coni_run(const pfg_input *in, const pfg_options *opt_in, pfg_output *
                 if (n_e) {
                     unsigned np2 = 1;
                     while (np2 < n_e) np2 <<= 1;
-                    WS(pept, W_PEPT, n_e * 4);
-                    WS(peg, W_PEG, n_e * 8);
-                    WS(pek0, W_PEK0, n_e * 8);
-                    WS(peord, W_PEORD, n_e * 4);
-                    WS(pkeep, W_PKEEP, (n_e + 1) * 8);
-                    WS(psort, W_PSORT, (size_t)np2 * 4);
+                    WSB(pept, W_PEPT, n_e * 4);
+                    WSB(peg, W_PEG, n_e * 8);
+                    WSB(pek0, W_PEK0, n_e * 8);
+                    WSB(peord, W_PEORD, n_e * 4);
+                    WSB(pkeep, W_PKEEP, (n_e + 1) * 8);
+                    WSB(psort, W_PSORT, (size_t)np2 * 4);
                     PA.e_pt = pept; PA.e_g = peg; PA.e_K0 = pek0; PA.e_ord = peord; PA.keep = pkeep;
                     k_pfv_fill<<<nsm * 4, 256>>>(PA); ++launches;
                     k_pfv_sort<<<1, 1024>>>(PA, n_e, np2, psort); ++launches;
@@ -688,9 +728,9 @@ static int coni_run(const pfg_input *in, const pfg_options *opt_in, pfg_output *
                 int herr[3] = {0, 0, 0};
                 if (n_pfv) {
                     int64_t *pK, *pM, *pP;
-                    WS(pK, W_PK, n_pfv * MH * 8);
-                    WS(pM, W_PM, n_pfv * MH * 8);
-                    WS(pP, W_PP, n_pfv * 8);
+                    WSB(pK, W_PK, n_pfv * MH * 8);
+                    WSB(pM, W_PM, n_pfv * MH * 8);
+                    WSB(pP, W_PP, n_pfv * 8);
                     k_pfv_rows<<<nsm * 8, 256>>>(PA, n_e, pK, pM, pP); ++launches;
                     CK(cudaGetLastError());
                     PfvChunk c{(int64_t *)pinned_get(n_pfv * MH * 8), (int64_t *)pinned_get(n_pfv * MH * 8),
@@ -714,11 +754,11 @@ static int coni_run(const pfg_input *in, const pfg_options *opt_in, pfg_output *
                     const double per = std::max((double)n_out / nb, W.rows_per_dir);
                     const size_t cap = std::max<size_t>(rows.n + n_out, (size_t)(per * (double)NP * 1.1) + 4096);
                     RowSink bigger;
-                    if (!bigger.alloc(cap)) { bigger.release(); set_err(out, "out of pinned host memory"); rc = 1; goto fail; }
+                    if (!bigger.alloc(cap, rw)) { bigger.release(); set_err(out, "out of pinned host memory"); rc = 1; goto fail; }
                     if (rows.n) {
                         CK(cudaStreamSynchronize(W.copy));
-                        memcpy(bigger.M, rows.M, rows.n * MH * 8);
-                        memcpy(bigger.Kn, rows.Kn, rows.n * MH * 8);
+                        memcpy(bigger.M, rows.M, rows.n * rw * 8);
+                        memcpy(bigger.Kn, rows.Kn, rows.n * rw * 8);
                         memcpy(bigger.q, rows.q, rows.n * 8);
                         memcpy(bigger.pidx, rows.pidx, rows.n * 8);
                         bigger.n = rows.n;
@@ -728,8 +768,8 @@ static int coni_run(const pfg_input *in, const pfg_options *opt_in, pfg_output *
                 }
                 CK(cudaEventRecord(W.rows_done[slot], 0));
                 CK(cudaStreamWaitEvent(W.copy, W.rows_done[slot], 0));
-                CK(cudaMemcpyAsync(rows.M + rows.n * MH, oM, n_out * MH * 8, cudaMemcpyDeviceToHost, W.copy));
-                CK(cudaMemcpyAsync(rows.Kn + rows.n * MH, oK, n_out * MH * 8, cudaMemcpyDeviceToHost, W.copy));
+                CK(cudaMemcpyAsync(rows.M + rows.n * rw, oM, n_out * rw * 8, cudaMemcpyDeviceToHost, W.copy));
+                CK(cudaMemcpyAsync(rows.Kn + rows.n * rw, oK, n_out * rw * 8, cudaMemcpyDeviceToHost, W.copy));
                 CK(cudaMemcpyAsync(rows.q + rows.n, oq, n_out * 8, cudaMemcpyDeviceToHost, W.copy));
                 CK(cudaMemcpyAsync(rows.pidx + rows.n, op, n_out * 8, cudaMemcpyDeviceToHost, W.copy));
                 CK(cudaEventRecord(W.copied[slot], W.copy));
@@ -774,6 +814,12 @@ static int coni_run(const pfg_input *in, const pfg_options *opt_in, pfg_output *
                     stats->points += (int64_t)npts;
                     stats->donated += (int64_t)(hctl[0].donated + hctl[1].donated);
                     stats->fp64_retries += (int64_t)retries;
+                    if (opt.check_fp32) {
+                        stats->fp32_rem_err = std::max(stats->fp32_rem_err, dbits(hctl[0].chk_rem));
+                        stats->fp32_margin_frac = std::max(stats->fp32_margin_frac, dbits(hctl[0].chk_frac));
+                        stats->fp32_end_err = std::max(stats->fp32_end_err, dbits(hctl[0].chk_end));
+                        stats->fp32_narrower += (int64_t)hctl[0].chk_narrower;
+                    }
                     stats->launches = launches;
                 }
                 if (in->verbose)
@@ -785,6 +831,22 @@ static int coni_run(const pfg_input *in, const pfg_options *opt_in, pfg_output *
             off += nb;
             ++sub;
         }
+        goto batches_done;
+    out_of_memory:
+        // out of device memory (another process, a partly filled GPU): free the
+        // per-batch buffers (copies in flight read the output slots: let them
+        // finish first), halve the batch and do the current batch again
+        cudaGetLastError();
+        if (W.copy) cudaStreamSynchronize(W.copy);
+        W.copy_pending[0] = W.copy_pending[1] = false;
+        ws_release(W, W_PS);                    // (the geometries' buffers stay)
+        batch = std::max<int64_t>(1, batch / 2);
+        pts_cap = std::max<unsigned long long>(1ull << 16, pts_cap / 2);
+        if (stats) stats->batch_retries++;
+        if (in->verbose) fprintf(stderr, "pfg: out of device memory at p %lld; batch -> %lld\n",
+                                 (long long)off, (long long)batch);
+        goto next_batches;
+    batches_done:;
     }
     if (in->verbose) fprintf(stderr, "pfg: [%.1f ms] all batches done\n", host_ms());
     CK(cudaStreamSynchronize(W.copy));

@@ -16,7 +16,8 @@
 //              thread per point: its place is its rank in its own run plus
 //              its rank in the partner run (binary search); log2 passes
 //   k_order    the sorted positions -> point indices
-//   k_rows     the MH-wide M and Kn rows, q and pidx in output order
+//   k_rows     the M and Kn rows (MH wide, or compact: the call's widest h11),
+//              q and pidx in output order
 //
 // The rows are exact in int64: the setup guarantees that every column of
 // Binter^T and (Z Binter)^T has an absolute sum below 2^31 (so each entry fits
@@ -287,7 +288,8 @@ struct RowArgs {
     int ks;
     unsigned long long n_out;
     int64_t pid_base;
-    int64_t *M, *Kn, *q, *pidx;   // output (n_out, MH), (n_out,)
+    int64_t *M, *Kn, *q, *pidx;   // output (n_out, rw), (n_out,)
+    int rw;                       // row width: MH, or the call's widest h11 (compact rows)
 };
 
 // one warp per output row: lanes own entries r = lane, lane + 32
@@ -322,9 +324,9 @@ __global__ void k_rows(RowArgs R)
                 if (lane + 32 < h) k1 += (int64_t)(int32_t)ZT[a * h + lane + 32] * ca;
             }
         }
-        int64_t *Mr = R.M + t * MH, *Kr = R.Kn + t * MH;
-        Mr[lane] = m0; Mr[lane + 32] = m1;
-        Kr[lane] = k0; Kr[lane + 32] = k1;
+        int64_t *Mr = R.M + t * R.rw, *Kr = R.Kn + t * R.rw;
+        if (lane < R.rw) { Mr[lane] = m0; Kr[lane] = k0; }
+        if (lane + 32 < R.rw) { Mr[lane + 32] = m1; Kr[lane + 32] = k1; }
         if (lane == 0) { R.q[t] = P.q; R.pidx[t] = R.pid_base + P.pid; }
     }
 }

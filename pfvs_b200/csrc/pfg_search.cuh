@@ -43,6 +43,9 @@ struct SearchCtl {
     int pad;
     unsigned long long npts;      // points emitted by all passes (see SearchArgs::npts)
     unsigned long long nodes, cands, leaves, donated;
+    // FP32 bound check (k_search_plain<float, NS, true>): maxima as the bit
+    // patterns of non-negative doubles, and a count
+    unsigned long long chk_rem, chk_frac, chk_end, chk_narrower;
 };
 
 struct SearchArgs {
@@ -136,10 +139,12 @@ template <class R> struct Prob {
     const R *U, *UI;                  // staged: U packed (upk), 1/U_ii
     const int32_t *MAT, *ZT;          // staged: mat (d x d), ZT (d x h)
     const int64_t *H;                 // global
+    const double *U64, *UI64;         // global: the FP64 factor (d x d row-major), 1/U_ii
     int d, h, m0_level, pad;
     int64_t g_lin, Q, qmax, linmin;
     uint64_t hrows;
     R qmax_r, slack, Kerr, max_err, invQ;
+    double slack_chol;                // the FP64 factor's certified margin (part of slack)
 };
 
 // Set up the problem of direction pid and stage its data in `stage` (the
@@ -170,12 +175,14 @@ template <class R> __device__ Prob<R> load_prob(const SearchArgs &A, int pid, vo
     P.d = d; P.h = h; P.m0_level = D.m0_level;
     P.g_lin = D.g_lin; P.Q = g.Q; P.qmax = g.qmax; P.linmin = g.linmin; P.hrows = D.hrows;
     P.U = U; P.UI = UI; P.MAT = MAT; P.ZT = ZT; P.H = s + L.H;
+    P.U64 = (const double *)(s + L.u64); P.UI64 = (const double *)(s + L.ui64);
     const R qd = (R)g.qmax;
     P.qmax_r = qd;
     // search constants (fpk_search_impl.h:30-39), plus the certified margin
     // of the FP64 Cholesky factor
     R sl = (R)A.eps > Num<R>::G() * (qd + (R)1) ? (R)A.eps : Num<R>::G() * (qd + (R)1);
     P.slack = sl + (R)D.slack_chol;
+    P.slack_chol = D.slack_chol;
     P.Kerr = (R)2 * (R)(D.d + 8) * Num<R>::U();
     P.max_err = sizeof(R) < sizeof(double) ? (R)1 + (R)0.05 * qd : (R)INFINITY;
     P.invQ = (R)1 / (R)g.Q;
@@ -277,27 +284,34 @@ template <class R, int NS> __device__ __forceinline__ void level_sums(const Lane
 // values: remaining norm rem, its error bound err, the gcd bound gab of the
 // rows above, the centre offset off and the absolute sum aoff
 // (fpk_search_impl.h:241-348).  Returns ST_RANGE if a bound leaves int32.
+// The real interval (a, b) of level i before rounding to integers (false:
+// the GCD bound rules the level out), in precision R with the constants
+// slack, Kerr, qmax and 1/U_ii given.
+template <class R> __device__ __forceinline__ bool level_interval(R slack, R Kerr, R qmax_r, int64_t Q, R ui, R rem,
+                                                                  R err, u128 gab, R off, R aoff, R &a, R &b)
+{
+    R Rr = sqrt(fmax(rem + slack + err, (R)0));
+    Rr += Kerr * (Rr + (R)2 * aoff) + Num<R>::tiny();
+    if (gab != 0 && (gab >> 64) == 0) {                 // GCD narrowing
+        R am = Rr + (R)2 * aoff;
+        R Rg2 = (R)Q * (R)(uint64_t)gab - (qmax_r - rem) + slack + err + Kerr * (am * am + rem);
+        if (Rg2 < (R)0) return false;
+        R Rg = sqrt(Rg2);
+        Rg += Kerr * (Rg + (R)2 * aoff) + Num<R>::tiny();
+        if (Rg < Rr) Rr = Rg;
+    }
+    a = (-Rr - off) * ui;
+    b = (Rr - off) * ui;
+    return true;
+}
+
 template <class R> __device__ __forceinline__ int level_range(const Prob<R> &P, int i, R rem, R err, u128 gab,
                                                               R off, R aoff, int64_t &lo_o, int64_t &hi_o)
 {
-    const R slack = P.slack, Kerr = P.Kerr;
-    R Rr = sqrt(fmax(rem + slack + err, (R)0));
-    Rr += Kerr * (Rr + (R)2 * aoff) + Num<R>::tiny();
-    bool empty = false;
-    if (gab != 0 && (gab >> 64) == 0) {                 // GCD narrowing
-        R am = Rr + (R)2 * aoff;
-        R Rg2 = (R)P.Q * (R)(uint64_t)gab - (P.qmax_r - rem) + slack + err + Kerr * (am * am + rem);
-        if (Rg2 < (R)0) empty = true;
-        else {
-            R Rg = sqrt(Rg2);
-            Rg += Kerr * (Rg + (R)2 * aoff) + Num<R>::tiny();
-            if (Rg < Rr) Rr = Rg;
-        }
-    }
+    R a = 0, b = 0;
+    const bool empty = !level_interval<R>(P.slack, P.Kerr, P.qmax_r, P.Q, P.UI[i], rem, err, gab, off, aoff, a, b);
     int64_t lo = 1, hi = 0;
     if (!empty) {
-        const R ui = P.UI[i];
-        R a = (-Rr - off) * ui, b = (Rr - off) * ui;
         a = ceil(a - Num<R>::G() * ((R)1 + fabs(a)));
         b = floor(b + Num<R>::G() * ((R)1 + fabs(b)));
         if (!(a >= -Num<R>::i32max() && b <= Num<R>::i32max())) return ST_RANGE;
@@ -361,9 +375,60 @@ template <class R, int NS> __device__ __forceinline__ void leaf_data(const Lanes
     B0 = shfl(S.y0, 0);
 }
 
-template <class R, int NS>
-__device__ int run_subtree(const SearchArgs &A, const Prob<R> &P, int pid, const WorkItem *it, Tally &T, int lane)
+// FP32-versus-FP64 bound check.  The FP32 search is run with an FP64 shadow
+// of its pruning quantities along the same path (the FP64 factor, FP64
+// sums): per candidate the FP32 remaining norm nr against the FP64 one
+// (abs difference, and its fraction of the FP32 safety margin slack + en
+// that the pruning test allows), per level the real interval endpoints
+// against the FP64 ones, and the levels whose FP32 integer range misses
+// part of the FP64 one.  FP64's own error is ~2^-29 of FP32's, so the FP64
+// values stand in for the exact ones.
+struct BoundAcc { double rem, frac, end; unsigned long long narrower; };
+struct Shadow64 { double rem0, rem1, err0, err1, off0, off1, aoff0, aoff1; };
+
+template <int NS> __device__ __forceinline__ void shadow_sums(const Lanes<float> &S, const Prob<float> &P, int i,
+                                                              int lane, double &off, double &aoff)
 {
+    const int d = P.d;
+    double o = 0, a = 0;
+    if (lane > i && lane < d) { const double t = P.U64[i * d + lane] * (double)S.c0; o += t; a += fabs(t); }
+    if (NS > 1 && lane + 32 > i && lane + 32 < d) {
+        const double t = P.U64[i * d + lane + 32] * (double)S.c1; o += t; a += fabs(t);
+    }
+    off = warp_sumr(o);
+    aoff = warp_sumr(a);
+}
+
+// the interval endpoints of level i in both precisions
+__device__ __forceinline__ void shadow_interval(const Prob<float> &P, int i, float rem, float err, u128 gab,
+                                                float off, float aoff, double rem64, double err64, double off64,
+                                                double aoff64, double slack64, double Kerr64, BoundAcc &acc)
+{
+    float a = 0, b = 0;
+    double a64 = 0, b64 = 0;
+    const bool ok32 = level_interval<float>(P.slack, P.Kerr, P.qmax_r, P.Q, P.UI[i], rem, err, gab, off, aoff, a, b);
+    const bool ok64 = level_interval<double>(slack64, Kerr64, (double)P.qmax, P.Q, P.UI64[i], rem64, err64, gab,
+                                             off64, aoff64, a64, b64);
+    if (ok32 && ok64) acc.end = fmax(acc.end, fmax(fabs((double)a - a64), fabs((double)b - b64)));
+    if (ok64) {
+        const double lo64 = ceil(a64 - Num<double>::G() * (1.0 + fabs(a64)));
+        const double hi64 = floor(b64 + Num<double>::G() * (1.0 + fabs(b64)));
+        if (lo64 <= hi64) {
+            if (!ok32) acc.narrower++;
+            else {
+                const float lo = ceil(a - Num<float>::G() * (1.0f + fabs(a)));
+                const float hi = floor(b + Num<float>::G() * (1.0f + fabs(b)));
+                if ((double)lo > lo64 || (double)hi < hi64) acc.narrower++;
+            }
+        }
+    }
+}
+
+template <class R, int NS, bool CHK = false>
+__device__ int run_subtree(const SearchArgs &A, const Prob<R> &P, int pid, const WorkItem *it, Tally &T, int lane,
+                           BoundAcc *acc = nullptr)
+{
+    static_assert(!CHK || sizeof(R) == 4, "the bound check shadows the FP32 search");
     const int d = P.d, h = P.h;
     Lanes<R> S;
     S.cur0 = S.cur1 = 0; S.hi0 = S.hi1 = -1;
@@ -377,12 +442,25 @@ __device__ int run_subtree(const SearchArgs &A, const Prob<R> &P, int pid, const
     R u_rem, u_err, u_off, u_aoff;
     u128 u_gab;
     i128 u_pre;
+    // FP32 bound check: the FP64 shadow of the current level and, per level, its owner's copy
+    Shadow64 SH{};
+    double w_rem = 0, w_err = 0, w_off = 0, w_aoff = 0;
+    double slack64 = 0, Kerr64 = 0;
+    if constexpr (CHK) {
+        slack64 = fmax(A.eps, Num<double>::G() * ((double)P.qmax + 1.0)) + P.slack_chol;
+        Kerr64 = 2.0 * (double)(d + 8) * Num<double>::U();
+    }
     if (!it) {                                    // the root of the direction
         top = i = d - 1;
         u_rem = P.qmax_r; u_err = P.Kerr * P.qmax_r; u_gab = 0;
         int st = enter_level<R, NS>(S, P, i, u_rem, u_err, u_gab, lane, u_cur, u_hi, u_off, u_aoff, u_pre);
         if (st) return st;
         T.nodes++;
+        if constexpr (CHK) {
+            w_rem = (double)P.qmax; w_err = Kerr64 * w_rem; w_off = 0; w_aoff = 0;
+            shadow_interval(P, i, u_rem, u_err, u_gab, u_off, u_aoff, w_rem, w_err, w_off, w_aoff, slack64, Kerr64, *acc);
+            LSET(SH, rem, i, w_rem); LSET(SH, err, i, w_err); LSET(SH, off, i, w_off); LSET(SH, aoff, i, w_aoff);
+        }
     } else {                                      // a donated node
         top = i = it->level;
         if (lane > i && lane < d) S.c0 = it->c[lane];
@@ -430,6 +508,10 @@ __device__ int run_subtree(const SearchArgs &A, const Prob<R> &P, int pid, const
                 u_off = LGET(S, off, i); u_aoff = LGET(S, aoff, i);
                 u_gab = shflu128((NS > 1 && i >= 32) ? S.gab1 : S.gab0, i & 31);
                 u_pre = shfl128((NS > 1 && i >= 32) ? S.pre1 : S.pre0, i & 31);
+                if constexpr (CHK) {
+                    w_rem = LGET(SH, rem, i); w_err = LGET(SH, err, i);
+                    w_off = LGET(SH, off, i); w_aoff = LGET(SH, aoff, i);
+                }
             }
 #ifdef PFG_STAGE_CLOCKS
             acc_bt += clock64() - k0;
@@ -490,11 +572,22 @@ __device__ int run_subtree(const SearchArgs &A, const Prob<R> &P, int pid, const
         R nr = 0, en = 0;
         u128 gn = gab;
         bool ferr = false;
+        double nr64 = 0, en64 = 0;
         if (pass) {
             R x = uii * (R)v + off;
             nr = rem - x * x;
             R ai = fabs(uii * (R)v) + aoff;
             en = err + Kerr * (ai * ai + rem);
+            if constexpr (CHK) {
+                const double u64 = P.U64[i * d + i];
+                const double x64 = u64 * (double)v + w_off;
+                nr64 = w_rem - x64 * x64;
+                const double ai64 = fabs(u64 * (double)v) + w_aoff;
+                en64 = w_err + Kerr64 * (ai64 * ai64 + w_rem);
+                const double dr = fabs((double)nr - nr64);
+                acc->rem = fmax(acc->rem, dr);
+                acc->frac = fmax(acc->frac, dr / ((double)slack + (double)en));
+            }
             if (en > P.max_err) { ferr = true; pass = false; }
             else if (nr < -(slack + en)) pass = false;
         }
@@ -546,6 +639,13 @@ __device__ int run_subtree(const SearchArgs &A, const Prob<R> &P, int pid, const
             int st = enter_level<R, NS>(S, P, i, u_rem, u_err, u_gab, lane, u_cur, u_hi, u_off, u_aoff, u_pre);
             if (st) return st;
             T.nodes++;
+            if constexpr (CHK) {
+                w_rem = shfl(nr64, t0); w_err = shfl(en64, t0);
+                shadow_sums<NS>(S, P, i, lane, w_off, w_aoff);
+                shadow_interval(P, i, u_rem, u_err, u_gab, u_off, u_aoff, w_rem, w_err, w_off, w_aoff, slack64,
+                                Kerr64, *acc);
+                LSET(SH, rem, i, w_rem); LSET(SH, err, i, w_err); LSET(SH, off, i, w_off); LSET(SH, aoff, i, w_aoff);
+            }
             if (i == 0) leaf_data<R, NS>(S, P, lane, A0, B0);
 #ifdef PFG_STAGE_CLOCKS
             acc_ds += clock64() - k1;
@@ -732,7 +832,7 @@ __global__ void __launch_bounds__(SEARCH_WARPS * 32, search_blocks<NS>()) k_sear
 
 // The plain form: one warp (block) per direction, no work sharing; pid < 0
 // takes the block's direction todo[blockIdx.x].
-template <class R, int NS>
+template <class R, int NS, bool CHK = false>
 __global__ void __launch_bounds__(32) k_search_plain(SearchArgs A, int pid)
 {
     if (pid < 0) {
@@ -749,8 +849,21 @@ __global__ void __launch_bounds__(32) k_search_plain(SearchArgs A, int pid)
     if (lane == 0) pending = A.dirs[pid].status == ST_PENDING;
     if (!shfl(pending, 0)) return;
     const Prob<R> P = load_prob<R>(A, pid, stage, lane);
-    int st = run_subtree<R, NS>(A, P, pid, nullptr, T, lane);
+    BoundAcc acc{0, 0, 0, 0};
+    int st = run_subtree<R, NS, CHK>(A, P, pid, nullptr, T, lane, &acc);
     finish_item<R>(A, pid, st, T, lane);
+    if constexpr (CHK) {
+        // the warp's maxima (each lane saw its own candidates), then the launch's
+        double m[3] = {acc.rem, acc.frac, acc.end};
+        for (int k = 0; k < 3; ++k)
+            for (int o = 16; o; o >>= 1) m[k] = fmax(m[k], __shfl_xor_sync(FULL, m[k], o));
+        if (lane == 0) {
+            atomicMax(&A.ctl->chk_rem, (unsigned long long)__double_as_longlong(m[0]));
+            atomicMax(&A.ctl->chk_frac, (unsigned long long)__double_as_longlong(m[1]));
+            atomicMax(&A.ctl->chk_end, (unsigned long long)__double_as_longlong(m[2]));
+            atomicAdd(&A.ctl->chk_narrower, acc.narrower);
+        }
+    }
 }
 
 }  // namespace pfg

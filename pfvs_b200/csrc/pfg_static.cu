@@ -5,8 +5,9 @@
 // Who needs it: callers that must not (or cannot) call cudaMalloc while they
 // run -- code inside a framework that owns all device memory through its own
 // pool or arena (an XLA/JAX custom call, a TensorRT plugin, an inference
-// server with a fixed budget), code on a stream that is being captured, or a
-// real-time path that may not block on the allocator.  They pass device
+// server with a fixed budget), where an allocation of its own would go around
+// that pool or fail, or a real-time path that may not block on the
+// allocator.  They pass device
 // buffers for the inputs and outputs; the scratch the kernels need (the
 // lattice setup's working arrays, the direction's lattice data, the search's
 // point staging and the sort indices) lives in g_static below, which every

@@ -47,7 +47,9 @@ class _Output(ctypes.Structure):
 class _Options(ctypes.Structure):
     _fields_ = [("form", ctypes.c_int), ("precision", ctypes.c_int),
                 ("blocks_per_sm", ctypes.c_int), ("warps_per_block", ctypes.c_int),
-                ("gcd_min_tree", ctypes.c_double)]
+                ("gcd_min_tree", ctypes.c_double), ("wait_s", ctypes.c_double),
+                ("deadline_s", ctypes.c_double), ("check_fp32", ctypes.c_int),
+                ("compact_rows", ctypes.c_int)]
 
 
 class _PfvOutput(ctypes.Structure):
@@ -61,7 +63,10 @@ class _Stats(ctypes.Structure):
                 ("leaves", ctypes.c_int64), ("points", ctypes.c_int64),
                 ("donated", ctypes.c_int64), ("fp64_retries", ctypes.c_int64),
                 ("ms_setup", ctypes.c_double), ("ms_search", ctypes.c_double),
-                ("ms_output", ctypes.c_double), ("launches", ctypes.c_int64)]
+                ("ms_output", ctypes.c_double), ("launches", ctypes.c_int64),
+                ("batch_retries", ctypes.c_int64), ("fp32_rem_err", ctypes.c_double),
+                ("fp32_margin_frac", ctypes.c_double), ("fp32_end_err", ctypes.c_double),
+                ("fp32_narrower", ctypes.c_int64)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -109,6 +114,7 @@ def _load():
     lib.pfg_coni_pfvs.restype = ctypes.c_int
     lib.pfg_pfv_output_free.argtypes = [ctypes.POINTER(_PfvOutput)]
     lib.pfg_release.argtypes = [ctypes.c_int]
+    lib.pfg_debug_fail_alloc.argtypes = [ctypes.c_int]
     _lib = lib
     return lib
 
@@ -149,6 +155,12 @@ def release(device: int = 0) -> None:
         lib.pfg_release(int(device))
 
 
+def debug_fail_alloc(k: int) -> None:
+    """Test hook: the k-th device allocation of the library from now on fails
+    once (out of memory), without allocating; k <= 0 cancels."""
+    _require().pfg_debug_fail_alloc(int(k))
+
+
 def max_h11() -> int:
     """The largest h11 the build supports (64)."""
     return _require().pfg_max_h11()
@@ -158,18 +170,31 @@ def _qmax(Q, dilation):
     return int(math.floor(dilation * Q + 1e-7))
 
 
+def _geometry_arrays(geoms, MH):
+    """pfg_input's per-geometry arrays: h11, Q, qmax = floor(dilation Q),
+    linmin = ceil(M0min), and the kappa and Mbasis blocks end to end."""
+    n_geo = len(geoms)
+    h = np.zeros(n_geo, dtype=np.int32)
+    Q, qmax, linmin = (np.zeros(n_geo, dtype=np.int64) for _ in range(3))
+    blocks_k, blocks_m = [], []
+    for k, g in enumerate(geoms):
+        kap_k = np.ascontiguousarray(g["kappa"], dtype=np.int64)
+        h[k] = kap_k.shape[0]
+        if not 3 <= h[k] <= MH:
+            raise ValueError(f"the GPU build supports 3 <= h11 <= {MH}")
+        Q[k] = int(g["Q"])
+        qmax[k] = _qmax(int(Q[k]), g["dilation"])
+        linmin[k] = math.ceil(g["M0min"] - 1e-9)
+        blocks_k.append(kap_k.reshape(-1))
+        blocks_m.append(np.ascontiguousarray(g["Mbasis"], dtype=np.int64).reshape(-1))
+    kap = np.concatenate(blocks_k) if blocks_k else np.zeros(1, dtype=np.int64)
+    Mb = np.concatenate(blocks_m) if blocks_m else np.zeros(1, dtype=np.int64)
+    return h, Q, qmax, linmin, kap, Mb
+
+
 def _pack(geoms, ps, pgeo, MH):
     n_geo = len(geoms)
-    h = np.array([np.asarray(g["kappa"]).shape[0] for g in geoms], dtype=np.int32)
-    if n_geo and (h.min() < 3 or h.max() > MH):
-        raise ValueError(f"the GPU build supports 3 <= h11 <= {MH}")
-    Q = np.array([int(g["Q"]) for g in geoms], dtype=np.int64)
-    qmax = np.array([_qmax(int(g["Q"]), g["dilation"]) for g in geoms], dtype=np.int64)
-    linmin = np.array([math.ceil(g["M0min"] - 1e-9) for g in geoms], dtype=np.int64)
-    kap = np.concatenate([np.ascontiguousarray(g["kappa"], dtype=np.int64).ravel() for g in geoms]) \
-        if n_geo else np.zeros(1, dtype=np.int64)
-    Mb = np.concatenate([np.ascontiguousarray(g["Mbasis"], dtype=np.int64).ravel() for g in geoms]) \
-        if n_geo else np.zeros(1, dtype=np.int64)
+    h, Q, qmax, linmin, kap, Mb = _geometry_arrays(geoms, MH)
     pgeo = np.ascontiguousarray(pgeo, dtype=np.int32)
     n_p = len(pgeo)
     if n_p and (np.any(pgeo < 0) or np.any(pgeo >= n_geo)):
@@ -234,13 +259,20 @@ def _view(owner, ptr, shape):
 
 def coni_batch_multi_ex(geoms, ps, pgeo, device=0, batch=0, verbose=False,
                         form=FORM_BATCHED, precision=PREC_AUTO, blocks_per_sm=0,
-                        warps_per_block=0, want_dir_nodes=False, gcd_min_tree=0.0):
+                        warps_per_block=0, want_dir_nodes=False, gcd_min_tree=0.0,
+                        wait_s=0.0, deadline_s=0.0, check_fp32=False, compact_rows=False):
     """
     `coni_batch_multi` with the search form (FORM_BATCHED: one persistent
     work-stealing launch; FORM_PLAIN: one warp per direction in one launch, FP64 pruning, no work sharing), the pruning
     precision (PREC_AUTO: the library's choice, FP64 on B200; PREC_FP64;
-    PREC_FP32: FP32 where qmax < 2^22 with an FP64 retry on -11) and the
-    call's statistics.  Returns
+    PREC_FP32: FP32 where qmax < 2^22 with an FP64 retry on -11), the
+    bounds on the search's waits (wait_s: a warp's wait for work, counted
+    from the launch, past which the call fails; deadline_s: one subtree's
+    search, past which its direction gets status -22; 0: 30 s and 120 s),
+    check_fp32 (with PREC_FP32: the FP32 pass with an FP64 shadow of its
+    pruning bounds; their errors in stats["fp32_*"]), compact_rows (M and
+    Kn rows as wide as the largest h11 of `geoms` instead of max_h11(): fewer
+    bytes copied back) and the call's statistics.  Returns
     (M, Kn, q, pidx, pstat, seconds_gpu, stats dict[, dir_nodes]).
     """
     lib = _require()
@@ -251,7 +283,8 @@ def coni_batch_multi_ex(geoms, ps, pgeo, device=0, batch=0, verbose=False,
                  kap.ctypes.data_as(_i64p), Mb.ctypes.data_as(_i64p),
                  n_p, P.ctypes.data_as(_i64p), pgeo.ctypes.data_as(_i32p),
                  int(device), int(batch), int(bool(verbose)))
-    opt = _Options(int(form), int(precision), int(blocks_per_sm), int(warps_per_block), float(gcd_min_tree))
+    opt = _Options(int(form), int(precision), int(blocks_per_sm), int(warps_per_block), float(gcd_min_tree),
+                   float(wait_s), float(deadline_s), int(bool(check_fp32)), int(bool(compact_rows)))
     st = _Stats()
     dn = np.zeros(max(n_p, 1), dtype=np.int64)
     out = _Output()
@@ -259,18 +292,23 @@ def coni_batch_multi_ex(geoms, ps, pgeo, device=0, batch=0, verbose=False,
                                ctypes.byref(st), dn.ctypes.data_as(_i64p))
     if rc != 0:
         raise RuntimeError(f"GPU pipeline failed: {out.err.decode(errors='replace')}")
-    # The row arrays view the library's (pinned) output buffers without a copy;
-    # the buffers go back to the library when the last view is collected.
+    width = max(3, int(h.max())) if (compact_rows and len(h)) else MH
+    res = _points(lib, out, n_p, width) + (st.as_dict(),)
+    return res + (dn[:n_p],) if want_dir_nodes else res
+
+
+def _points(lib, out, n_p, width):
+    """(M, Kn, q, pidx, pstat, seconds_gpu) of a filled pfg_output (rows of
+    `width` entries).  The row arrays view the library's (pinned) output
+    blocks without a copy; the blocks go back to the library when the last
+    view is collected."""
     owner = _OutputOwner(lib, out)
     n = out.n
-    M, Kn = _view(owner, out.M, (n, MH)), _view(owner, out.Kn, (n, MH))
+    M, Kn = _view(owner, out.M, (n, width)), _view(owner, out.Kn, (n, width))
     q, pidx = _view(owner, out.q, (n,)), _view(owner, out.pidx, (n,))
-    pstat = np.ctypeslib.as_array(out.pstat, shape=(n_p,)).copy() if n_p \
+    pstat = np.ctypeslib.as_array(out.pstat, shape=(n_p,)).astype(np.int8) if n_p \
         else np.zeros(0, dtype=np.int8)
-    secs = out.seconds_gpu
-    del owner
-    res = (M, Kn, q, pidx, pstat.astype(np.int8), secs, st.as_dict())
-    return res + (dn[:n_p],) if want_dir_nodes else res
+    return M, Kn, q, pidx, pstat, out.seconds_gpu
 
 
 class _PfvOwner:
@@ -304,7 +342,7 @@ def coni_pfvs_multi(geoms, ps, pgeo, device=0, batch=0, verbose=False, form=FORM
                  kap.ctypes.data_as(_i64p), Mb.ctypes.data_as(_i64p),
                  n_p, P.ctypes.data_as(_i64p), pgeo.ctypes.data_as(_i32p),
                  int(device), int(batch), int(bool(verbose)))
-    opt = _Options(int(form), int(precision), 0, 0, float(gcd_min_tree))
+    opt = _Options(int(form), int(precision), 0, 0, float(gcd_min_tree), 0.0, 0.0, 0, 0)
     st = _Stats()
     out = _PfvOutput()
     rc = lib.pfg_coni_pfvs(ctypes.byref(inp), ctypes.byref(opt), ctypes.byref(out), ctypes.byref(st))
@@ -326,7 +364,8 @@ def coni_pfvs_multi(geoms, ps, pgeo, device=0, batch=0, verbose=False, form=FORM
 def coni_batch_multi(geoms, ps, pgeo, device=0, batch=0, verbose=False):
     """
     The batched coni pipeline on the GPU for p-vectors of several geometries
-    at once (pfvs/gpu.py:136-211).
+    at once (pfvs/gpu.py:136-211), through the exported pfg_coni_batch (the
+    entry point the reference's loader binds).
 
     - `geoms`: per geometry a dict with `kappa` (h, h, h), `Mbasis` (h, h),
       `Q`, `dilation`, `M0min`.
@@ -339,7 +378,18 @@ def coni_batch_multi(geoms, ps, pgeo, device=0, batch=0, verbose=False):
     entries valid), q = c^T mat c, its p-vector index; points grouped by
     p-vector (ascending), sorted by (M, Kn) within one.
     """
-    return coni_batch_multi_ex(geoms, ps, pgeo, device, batch, verbose)[:6]
+    lib = _require()
+    MH = lib.pfg_max_h11()
+    h, Q, qmax, linmin, kap, Mb, P, pgeo, n_p = _pack(geoms, ps, pgeo, MH)
+    inp = _Input(len(geoms), h.ctypes.data_as(_i32p), Q.ctypes.data_as(_i64p),
+                 qmax.ctypes.data_as(_i64p), linmin.ctypes.data_as(_i64p),
+                 kap.ctypes.data_as(_i64p), Mb.ctypes.data_as(_i64p),
+                 n_p, P.ctypes.data_as(_i64p), pgeo.ctypes.data_as(_i32p),
+                 int(device), int(batch), int(bool(verbose)))
+    out = _Output()
+    if lib.pfg_coni_batch(ctypes.byref(inp), ctypes.byref(out)) != 0:
+        raise RuntimeError(f"GPU pipeline failed: {out.err.decode(errors='replace')}")
+    return _points(lib, out, n_p, MH)
 
 
 def coni_batch(kappa, Mbasis, ps, Q, dilation, M0min, max_N_out, device=0):
@@ -349,16 +399,16 @@ def coni_batch(kappa, Mbasis, ps, Q, dilation, M0min, max_N_out, device=0):
     ("more than max_N_pfvs outputs", as the reference kernel's status) and
     none of its points are returned.
     """
-    kappa = np.asarray(kappa)
-    h = kappa.shape[0]
     ps = np.asarray(ps, dtype=np.int64)
-    geoms = [dict(kappa=kappa, Mbasis=Mbasis, Q=Q, dilation=dilation, M0min=M0min)]
-    M, Kn, q, pidx, pstat, _ = coni_batch_multi(geoms, ps, np.zeros(len(ps), dtype=np.int32),
-                                                device=device)
-    counts = np.bincount(pidx, minlength=len(ps)) if len(pidx) else np.zeros(len(ps), dtype=np.int64)
-    over = counts > max_N_out
-    if np.any(over):
-        pstat[over] = -2
-        keep = ~over[pidx]
-        M, Kn, q, pidx = M[keep], Kn[keep], q[keep], pidx[keep]
-    return M[:, :h], Kn[:, :h], q, pidx, pstat
+    n_p = len(ps)
+    geom = {"kappa": kappa, "Mbasis": Mbasis, "Q": Q, "dilation": dilation, "M0min": M0min}
+    M, Kn, q, pidx, pstat, _ = coni_batch_multi([geom], ps, np.zeros(n_p, dtype=np.int32), device=device)
+    hh = np.asarray(kappa).shape[0]
+    rows_of = np.zeros(n_p, dtype=np.int64)
+    np.add.at(rows_of, pidx, 1)
+    too_many = np.flatnonzero(rows_of > max_N_out)
+    if too_many.size:
+        pstat[too_many] = -2
+        kept = ~np.isin(pidx, too_many)
+        M, Kn, q, pidx = M[kept], Kn[kept], q[kept], pidx[kept]
+    return M[:, :hh], Kn[:, :hh], q, pidx, pstat

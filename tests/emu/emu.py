@@ -38,6 +38,8 @@ def _load():
         lib.emu_output_free.argtypes = [ctypes.POINTER(gpu._Output)]
         lib.emu_witness_not_pd.argtypes = [ctypes.POINTER(ctypes.c_int64), ctypes.c_int]
         lib.emu_witness_not_pd.restype = ctypes.c_int
+        lib.emu_last_fp32_check.argtypes = [ctypes.POINTER(ctypes.c_double)]
+        lib.emu_set_gcd_min_tree.argtypes = [ctypes.c_double]
         _lib = lib
     return _lib
 
@@ -79,3 +81,18 @@ def witness_not_pd(A):
     lib = _load()
     A = np.ascontiguousarray(A, dtype=np.int64)
     return bool(lib.emu_witness_not_pd(A.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)), A.shape[0]))
+
+
+def last_fp32_check():
+    """After coni_batch_multi(..., precision=3) (FP32 pruning in the bound-check
+    form): dict of the FP32-versus-FP64 bound errors of that run."""
+    lib = _load()
+    b = (ctypes.c_double * 4)()
+    lib.emu_last_fp32_check(b)
+    return dict(rem_err=b[0], margin_frac=b[1], end_err=b[2], narrower=int(b[3]))
+
+
+def set_gcd_min_tree(v):
+    """GCD-row policy of the emulated setup, as pfg_options.gcd_min_tree
+    (0: the library default; < 0: rows for every direction)."""
+    _load().emu_set_gcd_min_tree(float(v))

@@ -28,10 +28,24 @@ template <class K> static void launch(unsigned grid, K kernel)
     for (unsigned b = 0; b < grid; ++b) emu_run_warp(b, 0, 32, grid, kernel);
 }
 
+// GCD-row policy of the emulated setup (pfg_options.gcd_min_tree's meaning after
+// the library maps it: 0 builds rows for every direction)
+static double g_emu_gcd_min_tree = GCD_MIN_TREE_DEFAULT;
+extern "C" void emu_set_gcd_min_tree(double v) { g_emu_gcd_min_tree = v < 0 ? 0.0 : (v == 0 ? GCD_MIN_TREE_DEFAULT : v); }
+
+// the last bound-check run's maxima (remaining-norm error, its fraction of the
+// FP32 margin, interval-endpoint error) and narrower-range count
+static double g_emu_chk[4];
+extern "C" void emu_last_fp32_check(double *out) { memcpy(out, g_emu_chk, sizeof g_emu_chk); }
+
+// precision: PFG_PREC_*, or 3 for FP32 pruning in the bound-check form
 extern "C" int emu_coni_batch(const pfg_input *in, int precision, int n_warps, pfg_output *out,
                               int64_t *dir_nodes_out, int32_t *dir_debug)
 {
     memset(out, 0, sizeof *out);
+    const bool check_fp32 = precision == 3;
+    if (check_fp32) precision = PFG_PREC_FP32;
+    memset(g_emu_chk, 0, sizeof g_emu_chk);
     const int64_t NP = in->n_p;
     std::vector<Geo> geos(in->n_geo);
     int64_t koff = 0, moff = 0;
@@ -66,7 +80,7 @@ extern "C" int emu_coni_batch(const pfg_input *in, int precision, int n_warps, p
     for (int k = 0; k < nb; ++k) (geos[pgeo[k]].h <= 32 ? o32 : o64).push_back(k);
     unsigned next64 = 0;
     SetupArgs SA{geos.data(), in->kappa, in->Mbasis, in->ps, pgeo.data(), slab_off.data(), slab.data(),
-                 dirs.data(), scratch.data(), (int)o32.size(), &next, o32.data(), 0, GCD_MIN_TREE_DEFAULT};
+                 dirs.data(), scratch.data(), (int)o32.size(), &next, o32.data(), 0, g_emu_gcd_min_tree};
     SetupArgs SA64 = SA;
     SA64.n = (int)o64.size(); SA64.next = &next64; SA64.todo = o64.data();
     fprintf(stderr, "emu: setup\n");
@@ -100,7 +114,19 @@ extern "C" int emu_coni_batch(const pfg_input *in, int precision, int n_warps, p
     int hmax = 3;
     for (int k = 0; k < nb; ++k) hmax = std::max(hmax, geos[pgeo[k]].h);
     const bool one = hmax <= 32;
-    if (!todo32.empty()) {
+    if (!todo32.empty() && check_fp32) {
+        // the FP32 bound-check form: one warp per direction with the FP64 shadow
+        SearchArgs C = A;
+        C.ctl = &ctl[0]; C.todo = todo32.data(); C.n_todo = (int)todo32.size(); C.pass = 1;
+        C.donate = 0; C.n_warps = 1;
+        launch((unsigned)todo32.size(), [&] {
+            if (one) k_search_plain<float, 1, true>(C, -1); else k_search_plain<float, 2, true>(C, -1);
+        });
+        double m[3];
+        memcpy(m, &ctl[0].chk_rem, sizeof m);
+        g_emu_chk[0] = m[0]; g_emu_chk[1] = m[1]; g_emu_chk[2] = m[2];
+        g_emu_chk[3] = (double)ctl[0].chk_narrower;
+    } else if (!todo32.empty()) {
         A.ctl = &ctl[0]; A.todo = todo32.data(); A.n_todo = (int)todo32.size(); A.pass = 1;
         launch(n_warps, [&] { if (one) k_search<float, 1>(A); else k_search<float, 2>(A); });
     }
@@ -144,7 +170,7 @@ extern "C" int emu_coni_batch(const pfg_input *in, int precision, int n_warps, p
         }
         launch(4, [&] { k_order(O, n_out, pin, sidx.data(), pout); });
         RowArgs R{dirs.data(), slab.data(), hdr.data(), coords.data(), sidx.data(), pout, keys.data(), ks, n_out, 0,
-                  out->M, out->Kn, out->q, out->pidx};
+                  out->M, out->Kn, out->q, out->pidx, MH};
         launch(4, [&] { k_rows(R); });
     }
     for (int k = 0; k < nb; ++k) {

@@ -140,6 +140,13 @@ template <class T, class U, class V> inline T atomicCAS(T *p, U cmp, V val)
     __atomic_compare_exchange_n(p, &c, (T)val, false, __ATOMIC_SEQ_CST, __ATOMIC_SEQ_CST);
     return c;
 }
+template <class T, class U> inline T atomicMax(T *p, U v)
+{
+    T cur = __atomic_load_n(p, __ATOMIC_SEQ_CST);
+    while (cur < (T)v && !__atomic_compare_exchange_n(p, &cur, (T)v, false, __ATOMIC_SEQ_CST, __ATOMIC_SEQ_CST)) {}
+    return cur;
+}
+inline long long __double_as_longlong(double x) { long long r; memcpy(&r, &x, sizeof r); return r; }
 
 using std::min;
 using std::max;

@@ -73,3 +73,45 @@ def test_input_packing_forms_agree_and_validate():
         gpu._pack(geoms, bad_list, pgeo, MH)
     with pytest.raises(ValueError):
         gpu._pack(geoms, full[:-1], pgeo, MH)
+
+
+def test_reference_loader_binds_this_library():
+    """The reference's own loader (pfvs/gpu.py, loaded by file path; it needs
+    only ctypes and numpy) binds this library through PFVS_GPU_LIB: its
+    struct layouts and the six entry points resolve, the constants come
+    through, and without a device its pipeline call ends in the library's
+    error (RuntimeError with the err string), not in a crash.  (On a GPU
+    machine the reference tree is absent; there the tests call the same
+    exported pfg_coni_batch through pfvs_b200.gpu.)"""
+    import ctypes
+    import importlib.util
+    import pytest
+    from conftest import REFERENCE
+    from pfvs_b200 import build, gpu
+    path = os.path.join(REFERENCE, "pfvs", "gpu.py")
+    if not os.path.exists(path):
+        pytest.skip("the reference tree is not present")
+    so = build.build()
+    old = os.environ.get("PFVS_GPU_LIB")
+    os.environ["PFVS_GPU_LIB"] = so
+    try:
+        spec = importlib.util.spec_from_file_location("reference_pfvs_gpu", path)
+        refmod = importlib.util.module_from_spec(spec)
+        spec.loader.exec_module(refmod)
+        assert refmod._load() is not None, refmod._lib_error
+        assert refmod.max_h11() == 64 and refmod.backend() == "cuda"
+        assert ctypes.sizeof(refmod._Input) == ctypes.sizeof(gpu._Input)
+        assert ctypes.sizeof(refmod._Output) == ctypes.sizeof(gpu._Output)
+        if not refmod.available():
+            import numpy as np
+            from pfvs_b200 import workloads
+            w = workloads.build("small", n_p=4)
+            g = w.geoms[0]
+            geoms = [dict(kappa=g.kappa, Mbasis=g.Mbasis, Q=g.Q, dilation=1.0, M0min=13)]
+            with pytest.raises(RuntimeError, match="GPU pipeline failed"):
+                refmod.coni_batch_multi(geoms, w.ps, np.zeros(len(w.ps), np.int32))
+    finally:
+        if old is None:
+            os.environ.pop("PFVS_GPU_LIB", None)
+        else:
+            os.environ["PFVS_GPU_LIB"] = old

@@ -1,0 +1,53 @@
+"""
+GPU: the FP32-versus-FP64 bound error, per configuration.
+
+The FP32-pruned search runs in its bound-check form (pfg_options.check_fp32:
+the same search with an FP64 shadow of its pruning quantities along the same
+path) over each configuration's full batch.  For every candidate tested and
+every level entered it records how far the FP32 remaining norm and interval
+endpoints are from the FP64 ones (FP64's own error being ~2^-29 of FP32's, the
+FP64 values stand in for the exact ones), what fraction of the FP32 pruning
+test's safety margin (slack + en, the rigorous error bound of
+fpk_search_impl.h:22-39 at unit roundoff 2^-24) that error uses, and the
+levels whose FP32 integer range misses part of the FP64 one.
+
+Required: the margin is never used up (fraction < 1), no level loses
+candidates against FP64, and the points are bit-identical to the FP64 form's.
+The figures are printed (and recorded as test properties) per configuration.
+"""
+import numpy as np
+import pytest
+
+from pfvs_b200 import gpu, workloads
+from parity import assert_same, layout
+
+pytestmark = pytest.mark.gpu
+
+CONFIGS = ["small", "plain", "mixed", "precision", "large"]
+
+
+@pytest.fixture(scope="module", autouse=True)
+def _built(lib):
+    if not gpu.available():
+        pytest.fail("no CUDA device: " + gpu.unavailable_reason())
+
+
+@pytest.mark.parametrize("name", CONFIGS)
+def test_fp32_bound_error(name, record_property):
+    w = workloads.build(name)
+    geoms, ps, pgeo, _ = layout(w)
+    chk = gpu.coni_batch_multi_ex(geoms, ps, pgeo, precision=gpu.PREC_FP32, check_fp32=True)
+    ref = gpu.coni_batch_multi_ex(geoms, ps, pgeo, precision=gpu.PREC_FP64)
+    st = chk[6]
+    fig = {k: st[k] for k in ("fp32_rem_err", "fp32_margin_frac", "fp32_end_err", "fp32_narrower",
+                              "fp64_retries")}
+    for k, v in fig.items():
+        record_property(k, v)
+    print(f"{name}: {len(ps)} directions, FP32 vs FP64: remaining norm {fig['fp32_rem_err']:.3e} "
+          f"({fig['fp32_margin_frac']:.4f} of the margin), endpoints {fig['fp32_end_err']:.3e}, "
+          f"narrower levels {fig['fp32_narrower']}, FP64 retries {fig['fp64_retries']}")
+    assert_same(chk, ref)
+    np.testing.assert_array_equal(chk[4], ref[4])
+    assert fig["fp32_narrower"] == 0
+    assert fig["fp32_margin_frac"] < 1.0
+    assert fig["fp32_rem_err"] > 0          # (the check ran)

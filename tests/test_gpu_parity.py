@@ -140,3 +140,21 @@ def test_batch_splits_give_identical_rows():
         assert_same(x, one)
         np.testing.assert_array_equal(x[4], one[4])
         assert x[6]["nodes"] == one[6]["nodes"]
+
+
+@pytest.mark.parametrize("name,n", [("mixed", 4096), ("precision", 64)])
+def test_compact_rows_equal_the_padded_rows(name, n):
+    """compact_rows: M and Kn rows as wide as the call's largest h11; the
+    entries equal the leading columns of the reference-layout rows (whose
+    other columns are zero)."""
+    w = workloads.build(name, n_p=n)
+    geoms, ps, pgeo, hs = layout(w)
+    full = gpu.coni_batch_multi_ex(geoms, ps, pgeo)
+    comp = gpu.coni_batch_multi_ex(geoms, ps, pgeo, compact_rows=True)
+    width = max(hs)
+    assert comp[0].shape[1] == width and comp[1].shape[1] == width
+    np.testing.assert_array_equal(comp[0], full[0][:, :width])
+    np.testing.assert_array_equal(comp[1], full[1][:, :width])
+    assert not full[0][:, width:].any() and not full[1][:, width:].any()
+    for a, b in zip(comp[2:5], full[2:5]):
+        np.testing.assert_array_equal(a, b)

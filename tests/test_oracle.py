@@ -206,3 +206,45 @@ def test_device_code_under_warp_emulator_on_dataset_geometries():
     assert np.all(got[4] == 0) and len(got[2]) > 20
     assert_same(got[:4], expected(geoms, ps, pgeo, "oracle"))
 
+
+
+def test_device_code_under_warp_emulator_with_gcd_rows_everywhere():
+    """The device search with GCD-cut rows built for every direction (the
+    reference's pruning): points equal the oracle's, and the rows prune
+    (fewer nodes than without them)."""
+    from emu import emu
+    w = workloads.build("mixed", n_p=96)
+    geoms, ps, pgeo, _ = layout(w)
+    sel = [3, 83, 85, 87]
+    ps, pgeo = [ps[i] for i in sel], pgeo[sel]
+    try:
+        emu.set_gcd_min_tree(-1.0)
+        rows = emu.coni_batch_multi(geoms, ps, pgeo, precision=1)
+        emu.set_gcd_min_tree(1e30)
+        none = emu.coni_batch_multi(geoms, ps, pgeo, precision=1)
+    finally:
+        emu.set_gcd_min_tree(0.0)
+    assert np.all(rows[4] == 0)
+    exp = expected(geoms, ps, pgeo, "oracle")
+    assert_same(rows[:4], exp)
+    assert_same(none[:4], exp)
+    assert rows[5].sum() < none[5].sum()
+
+
+def test_fp32_bound_check_under_warp_emulator():
+    """The FP32 search's bound-check form (an FP64 shadow of its pruning
+    quantities, pfg_options.check_fp32) on the emulated device: the FP32
+    remaining-norm error is a small part of the FP32 safety margin, no level's
+    FP32 range misses part of the FP64 one, and the points equal the FP64
+    form's."""
+    from emu import emu
+    for name, n, dils in (("mixed", 24, None),):
+        w = workloads.build(name, n_p=n, dilations=dils)
+        geoms, ps, pgeo, _ = layout(w)
+        a = emu.coni_batch_multi(geoms, ps, pgeo, precision=3)
+        chk = emu.last_fp32_check()
+        b = emu.coni_batch_multi(geoms, ps, pgeo, precision=1)
+        assert_same(a[:4], b[:4])
+        assert chk["narrower"] == 0
+        assert 0 < chk["margin_frac"] < 0.5
+        assert chk["rem_err"] > 0
