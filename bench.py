@@ -447,7 +447,28 @@ def main():
         d2h = rows * (2 * MH * 8 + 16) / args.steps + dirs / args.steps
         e2e = {"value": tot_nodes * args.steps / e2e_s, "unit": "nodes/s",
                "h2d_bytes_per_step": int(allsum(pg, h2d)), "d2h_bytes_per_step": int(allsum(pg, d2h)),
-               "ms_per_step": e2e_s / args.steps * 1e3}
+               "ms_per_step": e2e_s / args.steps * 1e3,
+               "path": "pfvs_b200.gpu.coni_batch_multi -> pfg_coni_batch (the reference's ABI: 64-wide rows)"}
+        # the same through the extension entry point with compact rows (as wide as the
+        # call's largest h11): the user-side option for fewer bytes copied back
+        wmax = max(int(np.asarray(g["kappa"]).shape[0]) for g in geoms)
+
+        def e2e_compact(k):
+            lo, hi = bounds[k]
+            out = gpu.coni_batch_multi_ex(geoms, ps[lo:hi], pgeo[lo:hi], device=device, compact_rows=True)
+            return len(out[2])
+        multi.run_chunks(queue("e2ec_warm"), len(bounds), e2e_compact)
+        barrier(pg)
+        t0 = time.perf_counter()
+        rows_c = 0
+        for s_ in range(args.steps):
+            rows_c += sum(multi.run_chunks(queue(f"e2ec{s_}"), len(bounds), e2e_compact).values())
+        e2ec_s = allmax(pg, time.perf_counter() - t0)
+        e2e["compact_rows"] = {"value": tot_nodes * args.steps / e2ec_s, "unit": "nodes/s",
+                               "ms_per_step": e2ec_s / args.steps * 1e3, "row_width": wmax,
+                               "d2h_bytes_per_step": int(allsum(pg, rows_c * (2 * wmax * 8 + 16) / args.steps
+                                                                + dirs / args.steps)),
+                               "path": "pfvs_b200.gpu.coni_batch_multi_ex(compact_rows=True) -> pfg_coni_batch_ex"}
     threads = os.cpu_count() or 1
     # CPU baseline: the reference kernel over the whole batch once (rank 0, N = 1)
     cpu = None
@@ -478,6 +499,14 @@ def main():
                                      "search": forms["plain"]["search_ms"] / per_step["ms_search"]}
         forms["batched_fp32_vs_plain"] = {"step": forms["plain"]["ms_per_step"] / forms["fp32"]["ms_per_step"],
                                           "search": forms["plain"]["search_ms"] / forms["fp32"]["search_ms"]}
+        # the FP32 pruning bounds against FP64 on this batch (the bound-check form, untimed)
+        rc_ = call(0, precision=gpu.PREC_FP32, check_fp32=True)
+        forms["fp32_bound_error"] = {k: rc_[6][k] for k in ("fp32_rem_err", "fp32_margin_frac", "fp32_end_err",
+                                                            "fp32_narrower")}
+        forms["fp32_bound_error"]["what"] = ("max over the FP32 pass of |FP32 - FP64| remaining norm (q units), its "
+                                             "fraction of the FP32 test's safety margin, interval endpoints "
+                                             "(coordinate units, including the FP32 margin's widening), and levels "
+                                             "whose FP32 range misses part of the FP64 one")
     # PFVs: the batch through the device post-processing (pfg_coni_pfvs), once,
     # untimed, and PFVs/s on the reference's dataset geometries (which have PFVs)
     pfv = None
