@@ -86,6 +86,7 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-extras", action="store_true", help="skip the forms and PFV figures")
+    ap.add_argument("--no-tune", action="store_true", help="the library's default grid and row policy")
     ap.add_argument("--chunk", type=int, default=8192, help="directions per queue chunk (N > 1)")
     return ap.parse_args()
 
@@ -381,13 +382,20 @@ def main():
         lo, hi = bounds[k]
         return gpu.coni_batch_multi_ex(geoms, ps[lo:hi], pgeo[lo:hi], device=device, **kw)
 
+    # the search grid and GCD-row policy from the autotuner (tuned on a sample of
+    # the batch, or read from its JSON store), untimed; they change time only
+    tuned = {}
+    if not args.no_tune and args.form == "batched":
+        from pfvs_b200 import tune
+        tuned = tune.autotune(geoms, ps, pgeo, device=device, n_sample=8192)
+
     # work unit: nodes of the FP64-pruned tree with every GCD-cut row built (the
     # reference's pruning), counted once, untimed; the timed steps build the
     # rows only where they pay off, which changes time but not the points.
     # Parity guard: the timed form returns the FP64 form's arrays.
     def unit(k):
         r64 = call(k, precision=gpu.PREC_FP64, gcd_min_tree=-1.0)
-        r = call(k, form=form, precision=prec)
+        r = call(k, form=form, precision=prec, **tuned)
         for a, b in zip(r[:5], r64[:5]):
             if not np.array_equal(a, b):
                 raise SystemExit("bench: timed form differs from the FP64 form")
@@ -400,7 +408,7 @@ def main():
         for k, v in g[2].items():
             failed[k] = failed.get(k, 0) + v
     for s_ in range(args.warmup):
-        multi.run_chunks(queue(f"warm{s_}"), len(bounds), lambda k: call(k, form=form, precision=prec)[5])
+        multi.run_chunks(queue(f"warm{s_}"), len(bounds), lambda k: call(k, form=form, precision=prec, **tuned)[5])
     # timed steps: device time (CUDA events inside the library)
     tot = dict(ms_setup=0.0, ms_search=0.0, ms_output=0.0, nodes=0, launches=0)
     failed_timed = {}
@@ -410,7 +418,7 @@ def main():
         t0 = time.perf_counter()
         for s_ in range(args.steps):
             def timed(k):
-                r = call(k, form=form, precision=prec)
+                r = call(k, form=form, precision=prec, **tuned)
                 for key in tot:
                     tot[key] += r[6][key]
                 for st_, v in failed_by_status(r[4]).items():
@@ -556,6 +564,7 @@ def main():
                 "data": "synthetic (seeded CY instances, pfvs_b200/workloads.py)",
                 "config": {"workload": workload_desc(args, w),
                            "form": args.form, "precision": args.precision,
+                           "tuned_options": tuned or "library defaults",
                            "directions_per_gpu": len(idx) // world,
                            "l2": "working set per step > 126 MB (slabs + points); no flush needed",
                            "parallelism": (f"directions in chunks of {bounds[0][1]} pulled by {world} GPUs "
