@@ -18,7 +18,9 @@
 // candidates at once and a ballot picks the next child (DFS order) or the
 // passing leaves.  The exact sums mat c and ZB c are kept per lane
 // (lane r owns rows r, r+32) and updated by one column whenever a coordinate
-// changes, so a leaf costs O(1) exact work.  (M = Binter c is formed after
+// changes, so a leaf costs O(1) exact work; the GCD rows' prefixes
+// (H_r c over the coordinates above row r's pivot, lane r) are kept the
+// same way, with the column of H that a coordinate change touches.  (M = Binter c is formed after
 // the search from the emitted c.)  Warps take whole directions
 // from a counter and donate the top of their DFS stack to a global queue
 // when other warps run out of work (persistent kernel, work stealing).
@@ -124,21 +126,25 @@ template <> struct Num<double> {
 
 // The search data of one direction, staged by the warp that searches it:
 // U packed by rows (upper triangle, row i holds U[i][i..d-1]), 1/U_ii, and
-// mat and ZB^T as int32 (the setup bounds their row / column absolute sums by 2^31); the
-// GCD-cut rows H stay in global memory (only large trees have them).
+// mat and ZB^T as int32 (the setup bounds their row / column absolute sums by 2^31), and
+// the GCD rows' pivots H_ii; the GCD-cut rows H themselves stay in global memory (only
+// large trees have them), read one column per coordinate change.
 PFG_HD int upk(int i, int j, int d) { return i * d - ((i * (i - 1)) >> 1) + (j - i); }
 template <class R> PFG_HD unsigned stage_bytes(int d, int h)
 {
     unsigned b = (unsigned)((d * (d + 1) / 2 + d) * sizeof(R));
     b = (b + 15u) & ~15u;
     b += (unsigned)(d * d + d * h) * 4u;
+    b = (b + 15u) & ~15u;
+    b += (unsigned)d * 8u;                      // H_ii
     return (b + 15u) & ~15u;
 }
 
 template <class R> struct Prob {
     const R *U, *UI;                  // staged: U packed (upk), 1/U_ii
     const int32_t *MAT, *ZT;          // staged: mat (d x d), ZT (d x h)
-    const int64_t *H;                 // global
+    const int64_t *HD;                // staged: the GCD rows' pivots H_ii (0 where no row is kept)
+    const int64_t *H;                 // global, transposed: H[c d + r] = entry c of the row with pivot r
     const double *U64, *UI64;         // global: the FP64 factor (d x d row-major), 1/U_ii
     int d, h, m0_level, pad;
     int64_t g_lin, Q, qmax, linmin;
@@ -162,6 +168,8 @@ template <class R> __device__ Prob<R> load_prob(const SearchArgs &A, int pid, vo
     R *U = (R *)stage, *UI = U + d * (d + 1) / 2;
     int32_t *MAT = (int32_t *)((char *)stage + ((((d * (d + 1) / 2 + d) * sizeof(R)) + 15) & ~(size_t)15));
     int32_t *ZT = MAT + d * d;
+    int64_t *HD = (int64_t *)((char *)stage + ((((((d * (d + 1) / 2 + d) * sizeof(R)) + 15) & ~(size_t)15)
+                                                 + (size_t)(d * d + d * h) * 4 + 15) & ~(size_t)15));
     __syncwarp();                                   // (the previous problem's readers are done)
     for (int e = lane; e < d * d; e += 32) {
         const int i = e / d, j = e - i * d;
@@ -170,11 +178,12 @@ template <class R> __device__ Prob<R> load_prob(const SearchArgs &A, int pid, vo
     }
     for (int e = lane; e < d; e += 32) UI[e] = UIg[e];
     for (int e = lane; e < d * h; e += 32) ZT[e] = (int32_t)ZTg[e];
+    for (int e = lane; e < d; e += 32) HD[e] = ((D.hrows >> e) & 1) ? s[L.H + (int64_t)e * d + e] : 0;
     __syncwarp();
     Prob<R> P;
     P.d = d; P.h = h; P.m0_level = D.m0_level;
     P.g_lin = D.g_lin; P.Q = g.Q; P.qmax = g.qmax; P.linmin = g.linmin; P.hrows = D.hrows;
-    P.U = U; P.UI = UI; P.MAT = MAT; P.ZT = ZT; P.H = s + L.H;
+    P.U = U; P.UI = UI; P.MAT = MAT; P.ZT = ZT; P.HD = HD; P.H = s + L.H;
     P.U64 = (const double *)(s + L.u64); P.UI64 = (const double *)(s + L.ui64);
     const R qd = (R)g.qmax;
     P.qmax_r = qd;
@@ -234,7 +243,7 @@ template <class R> struct Lanes {
     int64_t cur0, cur1, hi0, hi1;
     R rem0, rem1, err0, err1, off0, off1, aoff0, aoff1;
     u128 gab0, gab1;              // gcd of the rows above the level
-    i128 pre0, pre1;              // GCD-row prefix at the level
+    i128 hp0, hp1;                // H_r c over c[r+1:], r = lane, lane+32 (the GCD row's prefix)
     int32_t c0, c1;               // c[lane], c[lane+32]
     int64_t y0, y1;               // (mat c)_r, r = lane, lane+32, over c[1:]
     int64_t k0, k1;               // (ZB c)_r over c[1:]
@@ -243,7 +252,8 @@ template <class R> struct Lanes {
 #define LGET(S, f, i) shfl((NS > 1 && (i) >= 32) ? S.f##1 : S.f##0, (i) & 31)
 #define LSET(S, f, i, val) do { if (lane == ((i) & 31)) { if (NS > 1 && (i) >= 32) S.f##1 = (val); else S.f##0 = (val); } } while (0)
 
-// c[i] changes by dv (i >= 1): update the exact incremental sums
+// c[i] changes by dv (i >= 1): update the exact incremental sums (the GCD
+// rows' prefixes of the levels below i with column i of H)
 template <class R, int NS> __device__ __forceinline__ void apply_dc(Lanes<R> &S, const Prob<R> &P, int i, int64_t dv, int lane)
 {
     if (dv == 0 || i == 0) return;
@@ -252,6 +262,8 @@ template <class R, int NS> __device__ __forceinline__ void apply_dc(Lanes<R> &S,
     if (NS > 1 && lane + 32 < d) S.y1 += (int64_t)P.MAT[i * d + lane + 32] * dv;
     if (lane < h) S.k0 += (int64_t)P.ZT[i * h + lane] * dv;
     if (NS > 1 && lane + 32 < h) S.k1 += (int64_t)P.ZT[i * h + lane + 32] * dv;
+    if (lane < i && ((P.hrows >> lane) & 1)) S.hp0 += (i128)P.H[i * d + lane] * dv;
+    if (NS > 1 && lane + 32 < i && ((P.hrows >> (lane + 32)) & 1)) S.hp1 += (i128)P.H[i * d + lane + 32] * dv;
 }
 
 // the dot products of entering level i (c[i+1:] set): off, aoff, GCD prefix
@@ -260,24 +272,21 @@ template <class R, int NS> __device__ __forceinline__ void level_sums(const Lane
 {
     const int d = P.d;
     R o = 0, a = 0;
-    i128 pr = 0;
     const bool hrow = (P.hrows >> i) & 1;
     const R *Ui = P.U + upk(i, i, d) - i;           // Ui[j] = U[i][j], j >= i
     int j = lane;
     if (j > i && j < d) {
         R t = Ui[j] * (R)S.c0;
         o += t; a += fabs(t);
-        if (hrow) pr += (i128)P.H[i * d + j] * S.c0;
     }
     j = lane + 32;
     if (NS > 1 && j > i && j < d) {
         R t = Ui[j] * (R)S.c1;
         o += t; a += fabs(t);
-        if (hrow) pr += (i128)P.H[i * d + j] * S.c1;
     }
     off = warp_sumr(o);
     aoff = warp_sumr(a);
-    pre = hrow ? warp_sum128(pr) : (i128)0;
+    pre = hrow ? shfl128((NS > 1 && i >= 32) ? S.hp1 : S.hp0, i & 31) : (i128)0;
 }
 
 // The candidate range [lo, hi] (lo > hi: none) of level i from its entry
@@ -359,7 +368,7 @@ template <class R, int NS> __device__ int enter_level(Lanes<R> &S, const Prob<R>
     LSET(S, cur, i, lo); LSET(S, hi, i, hi);
     LSET(S, rem, i, rem); LSET(S, err, i, err);
     LSET(S, off, i, off); LSET(S, aoff, i, aoff);
-    LSET(S, gab, i, gab); LSET(S, pre, i, pre);
+    LSET(S, gab, i, gab);
     lo_o = lo; hi_o = hi;
     return 0;
 }
@@ -433,7 +442,7 @@ __device__ int run_subtree(const SearchArgs &A, const Prob<R> &P, int pid, const
     Lanes<R> S;
     S.cur0 = S.cur1 = 0; S.hi0 = S.hi1 = -1;
     S.rem0 = S.rem1 = S.err0 = S.err1 = S.off0 = S.off1 = S.aoff0 = S.aoff1 = 0;
-    S.gab0 = S.gab1 = 0; S.pre0 = S.pre1 = 0;
+    S.gab0 = S.gab1 = 0; S.hp0 = S.hp1 = 0;
     S.c0 = S.c1 = 0; S.y0 = S.y1 = S.k0 = S.k1 = 0;
     int top, i;
     // The current level's entry values, the same in every lane (its owner
@@ -477,7 +486,7 @@ __device__ int run_subtree(const SearchArgs &A, const Prob<R> &P, int pid, const
         LSET(S, cur, i, it->cur); LSET(S, hi, i, it->hi);
         LSET(S, rem, i, (R)it->rem); LSET(S, err, i, (R)it->err);
         LSET(S, off, i, off); LSET(S, aoff, i, aoff);
-        LSET(S, gab, i, gab); LSET(S, pre, i, pre);
+        LSET(S, gab, i, gab);
         u_cur = it->cur; u_hi = it->hi; u_rem = (R)it->rem; u_err = (R)it->err;
         u_off = off; u_aoff = aoff; u_gab = gab; u_pre = pre;
     }
@@ -507,7 +516,8 @@ __device__ int run_subtree(const SearchArgs &A, const Prob<R> &P, int pid, const
                 u_rem = LGET(S, rem, i); u_err = LGET(S, err, i);
                 u_off = LGET(S, off, i); u_aoff = LGET(S, aoff, i);
                 u_gab = shflu128((NS > 1 && i >= 32) ? S.gab1 : S.gab0, i & 31);
-                u_pre = shfl128((NS > 1 && i >= 32) ? S.pre1 : S.pre0, i & 31);
+                // (H_i c over c[i+1:] has not changed since level i was entered)
+                u_pre = ((P.hrows >> i) & 1) ? shfl128((NS > 1 && i >= 32) ? S.hp1 : S.hp0, i & 31) : (i128)0;
                 if constexpr (CHK) {
                     w_rem = LGET(SH, rem, i); w_err = LGET(SH, err, i);
                     w_off = LGET(SH, off, i); w_aoff = LGET(SH, aoff, i);
@@ -564,7 +574,7 @@ __device__ int run_subtree(const SearchArgs &A, const Prob<R> &P, int pid, const
         const u128 gab = u_gab;
         const i128 pre = u_pre;
         const bool hrow = (P.hrows >> i) & 1;
-        const int64_t hii = hrow ? P.H[i * d + i] : 0;
+        const int64_t hii = P.HD[i];
         const R uii = P.U[upk(i, i, d)];
         const int64_t ncand = min((int64_t)32, hi - cur + 1);
         const int64_t v = cur + lane;

@@ -1071,7 +1071,9 @@ template <int N> __device__ int setup_phase2(const SetupArgs &A, int pid, int la
                 for (int c = lane; c < d; c += 32) fits &= uabs64(S->B[(nr - 1) * N + c]) < (1ull << 62);
                 fits = __all_sync(FULL, fits);
                 if (fits) {
-                    for (int c = lane; c < d; c += 32) H[col * d + c] = S->B[(nr - 1) * N + c];
+                    // stored transposed (H[c d + col] = entry c of the row with pivot col): the
+                    // search updates every row's prefix with column c when coordinate c changes
+                    for (int c = lane; c < d; c += 32) H[c * d + col] = S->B[(nr - 1) * N + c];
                     hrows |= 1ull << col;
                 }
                 __syncwarp();

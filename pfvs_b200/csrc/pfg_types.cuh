@@ -50,7 +50,8 @@ struct Dir {
 //   BT   d x h  int64   Binter^T: BT[a][r] = Binter[r][a]
 //   ZT   d x h  int64   (Z Binter)^T
 //   MAT  d x d  int64   ellipsoid matrix
-//   H    d x d  int64   GCD rows: row j has its first nonzero at column j
+//   H    d x d  int64   GCD rows, transposed: H[c d + j] = entry c of the row whose
+//                        first nonzero is at column j
 //   U64  d x d  double  upper Cholesky factor (U^T U = mat + a certified perturbation)
 //   U32  d x d  float   U64 rounded to float (padded to whole words)
 //   UI64 d      double  1 / U64[i][i]

@@ -50,4 +50,6 @@ def test_fp32_bound_error(name, record_property):
     np.testing.assert_array_equal(chk[4], ref[4])
     assert fig["fp32_narrower"] == 0
     assert fig["fp32_margin_frac"] < 1.0
-    assert fig["fp32_rem_err"] > 0          # (the check ran)
+    # (the check ran: configurations 1 and 2 at dilation 1 have trees of a few
+    # nodes whose FP32 remaining norms happen to be exact; their endpoints still differ)
+    assert fig["fp32_rem_err"] > 0 or fig["fp32_end_err"] > 0

@@ -115,7 +115,7 @@ def test_static_entry_reports_too_many_points(caller):
     """A direction with k points, called with room for k - 1: status -2 and no
     rows (the batch entry point's own count decides k)."""
     torch = caller.torch
-    w = workloads.build("plain", n_p=48, dilations=(150.0,))
+    w = workloads.build("mixed", n_p=96)
     geoms, ps, pgeo, _ = layout(w)
     M, Kn, q, pidx, pstat, _ = gpu.coni_batch_multi(geoms, ps, pgeo)
     counts = np.bincount(pidx, minlength=len(ps))
