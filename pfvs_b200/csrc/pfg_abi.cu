@@ -60,7 +60,8 @@ enum {
     W_GEO, W_KAPPA, W_MB, W_PS, W_PGEO, W_SLABOFF, W_SLAB, W_DIRS, W_SCRATCH, W_TODO32, W_TODOALL, W_ORDER,
     W_CTL, W_ITEMS, W_READY, W_HDR, W_COORDS, W_DIRNODES, W_DIRPASS,
     W_KEYS, W_COUNT, W_FILL, W_SEG, W_IDX, W_CSEG, W_SUM, W_PERM, W_PERM2, W_SIDX, W_PCNT, W_PKG, W_PEPT, W_PEG, W_PEK0, W_PEORD, W_PNONS, W_PKEEP,
-    W_PERR, W_PSORT, W_PK, W_PM, W_PP, W_PRIMES, W_OM, W_OK, W_OQ, W_OP, W_OM2, W_OK2, W_OQ2, W_OP2, W_RETRY, W_N
+    W_PERR, W_PSORT, W_PK, W_PM, W_PP, W_PRIMES, W_OM, W_OK, W_OQ, W_OP, W_OM2, W_OK2, W_OQ2, W_OP2, W_RETRY,
+    W_ROWS, W_N
 };
 
 struct Workspace {
@@ -465,6 +466,7 @@ static int coni_run(const pfg_input *in, const pfg_options *opt_in, pfg_output *
                 CK(cudaFuncSetAttribute(k_setup<32, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem32));
                 CK(cudaFuncSetAttribute(k_setup<32, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem32));
                 CK(cudaFuncSetAttribute(k_setup<32, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem32));
+                CK(cudaFuncSetAttribute(k_setup<32, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem32));
                 int bpsm = 0;
                 CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bpsm, k_setup<32, 1>, 32, smem32));
                 grid32 = std::min(n32, nsm * std::max(1, bpsm));
@@ -496,6 +498,8 @@ static int coni_run(const pfg_input *in, const pfg_options *opt_in, pfg_output *
             WSB(ddirnodes, W_DIRNODES, (size_t)nb * 8);
             WSB(ddirpass, W_DIRPASS, (size_t)nb * 4);
             WSB(dretry, W_RETRY, 64);
+            int32_t *drows;
+            WSB(drows, W_ROWS, (size_t)nb * 4);
             CK(cudaMemcpy(dps, &in->ps[off * MH], (size_t)nb * MH * 8, cudaMemcpyHostToDevice));
             CK(cudaMemcpy(dpgeo, &in->pgeo[off], (size_t)nb * 4, cudaMemcpyHostToDevice));
             CK(cudaMemcpy(dslaboff, slab_off.data(), (size_t)nb * 8, cudaMemcpyHostToDevice));
@@ -515,12 +519,14 @@ static int coni_run(const pfg_input *in, const pfg_options *opt_in, pfg_output *
             // ---- setup ----
             CK(cudaEventRecord(ev[0]));
             {
+                // work counters: [0..2] phases 0-2 (h11 <= 32), [3..5] (h11 > 32), [6], [7]
+                // phase 3; [8], [9] the lengths of the two GCD-row queues phase 2 fills
                 unsigned *counters = (unsigned *)((char *)dctl + 2 * sizeof(SearchCtl));
                 // phases in order, each over all directions (one work counter per launch)
                 SetupArgs SA32{dgeo, dkappa, dmb, dps, dpgeo, dslaboff, dslab, ddirs, dscr, n32,
-                               counters, dorder, 1, gcd_min_tree};
+                               counters, dorder, 1, gcd_min_tree, drows, counters + 8, nullptr};
                 SetupArgs SA64{dgeo, dkappa, dmb, dps, dpgeo, dslaboff, dslab, ddirs, dscr, n64,
-                               counters + 3, dorder + n32, 0, gcd_min_tree};
+                               counters + 3, dorder + n32, 0, gcd_min_tree, drows + n32, counters + 9, nullptr};
                 if (n32) { k_setup<32, 0><<<grid32, 32, smem32>>>(SA32); ++launches; }
                 if (n64) { k_setup<MH, 0><<<grid64[0], 128>>>(SA64); ++launches; }
                 SA32.next = counters + 1; SA64.next = counters + 4;
@@ -529,6 +535,11 @@ static int coni_run(const pfg_input *in, const pfg_options *opt_in, pfg_output *
                 SA32.next = counters + 2; SA64.next = counters + 5;
                 if (n32) { k_setup<32, 2><<<grid32, 32, smem32>>>(SA32); ++launches; }
                 if (n64) { k_setup<MH, 2><<<grid64[2], 128>>>(SA64); ++launches; }
+                // phase 3: the GCD rows of the queued (large-tree) directions, all at once
+                SA32.next = counters + 6; SA32.todo = drows; SA32.n_dev = counters + 8;
+                SA64.next = counters + 7; SA64.todo = drows + n32; SA64.n_dev = counters + 9;
+                if (n32) { k_setup<32, 3><<<grid32, 32, smem32>>>(SA32); ++launches; }
+                if (n64) { k_setup<MH, 3><<<grid64[2], 128>>>(SA64); ++launches; }
                 CK(cudaGetLastError());
             }
             CK(cudaEventRecord(ev[1]));

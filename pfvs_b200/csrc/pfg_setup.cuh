@@ -84,6 +84,11 @@ struct SetupArgs {
     int smem_core;                          // 1: the LllMem<32> lives in dynamic shared memory
     double gcd_min_tree;                    // GCD rows only for trees estimated at >= this many
                                             // nodes (<= 0: always)
+    // split form (the batched path): phase 2 queues the directions that want GCD
+    // rows into rows_list (rows_count entries) for phase 3; null: phase 2 builds them
+    int32_t *rows_list;
+    unsigned *rows_count;
+    const unsigned *n_dev;                  // if set, the number of todo entries (device)
 };
 
 // Per-stage cycle accounting of the setup, compiled in only with
@@ -688,7 +693,11 @@ __device__ bool witness_not_pd(const int64_t *A, int d, double *U, double *y, in
 // set (N >= h11).  Each returns ST_PENDING to go on, else the final status.
 //   phase 0: steps 1-7 (Z, v, orthogonal lattice, Euclidean LLL, Binter, mat)
 //   phase 1: step 8 (cut-aware basis)
-//   phase 2: steps 10, 9, 11 (Cholesky and certificate, GCD rows, bounds)
+//   phase 2: step 10 (Cholesky and certificate, tree estimate), then 9 and 11
+//            (GCD rows, bounds) -- or, in the split form, 11 only for the
+//            directions without GCD rows, the others queued for
+//   phase 3: steps 9 and 11 of the queued directions (the GCD rows of the
+//            large trees then run side by side instead of trailing phase 2)
 // ---------------------------------------------------------------------------
 template <int N> __device__ int setup_phase0(const SetupArgs &A, int pid, int lane, int &stage, LllMem<N> *S)
 {
@@ -892,103 +901,21 @@ template <int N> __device__ int setup_phase1(const SetupArgs &A, int pid, int la
     return ST_PENDING;
 }
 
-template <int N> __device__ int setup_phase2(const SetupArgs &A, int pid, int lane, int &stage, LllMem<N> *S)
+// Steps 9 and 11 of one direction: its GCD rows (when wanted) and the int64
+// bounds of the search's sums.
+template <int N> __device__ int setup_rows_bounds(const SetupArgs &A, int pid, int lane, int &stage, LllMem<N> *S,
+                                                  bool want_rows, double slack_chol)
 {
     SetupScratch *W = A.scratch + (blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5));
     const Geo g = A.geo[A.pgeo[pid]];
     const int h = g.h, d = h - 1;
-    const int64_t *kap = A.kappa + g.koff, *Mb = A.Mbasis + g.moff, *p = A.ps + (int64_t)pid * MH;
+    const int64_t *p = A.ps + (int64_t)pid * MH;
     int64_t *slab = A.slab + A.slab_off[pid];
     const Slab L = slab_layout(h, d);
     Dir &D = A.dirs[pid];
     bool bad = false;
     StageClock clk(stage, lane);
-    (void)kap; (void)Mb;
     int64_t *BT = slab + L.bt, *ZT = slab + L.zt, *MAT = slab + L.mat;
-    const int m0_level = D.m0_level;
-    const int64_t g_lin = D.g_lin;
-    clk.mark(10);
-    // 10. FP64 Cholesky of mat, certificate, float copies
-    double *U = (double *)(slab + L.u64);
-    for (int e = lane; e < d * d; e += 32) U[e] = 0.0;
-    __syncwarp();
-    bool notpd = false;
-    for (int j = 0; j < d; ++j) {
-        // row j of U: U_jj = sqrt(A_jj - sum_{k<j} U_kj^2), U_ji = (A_ji - sum_k U_kj U_ki) / U_jj
-        double s0 = 0.0;
-        for (int k = 0; k < j; ++k) { double u = U[k * d + j]; s0 += u * u; }
-        double pj = (double)MAT[j * d + j] - s0;
-        if (!(pj > 0)) { notpd = true; break; }
-        double ujj = sqrt(pj);
-        for (int i = j + 1 + lane; i < d; i += 32) {
-            double s = 0.0;
-            for (int k = 0; k < j; ++k) s += U[k * d + j] * U[k * d + i];
-            U[j * d + i] = ((double)MAT[j * d + i] - s) / ujj;
-        }
-        if (lane == 0) U[j * d + j] = ujj;
-        __syncwarp();
-    }
-    if (notpd)                               // not positive definite, or not decided here
-        return witness_not_pd(MAT, d, U, W->X, lane) ? ST_NOT_PD : ST_PRECISION;
-    // ||U||_F^2 and ||U^-1||_F^2
-    double *X = W->X;
-    for (int j = 0; j < d; ++j) {
-        for (int i = lane; i <= j; i += 32) {
-            double x;
-            if (i == j) x = 1.0 / U[j * d + j];
-            else {
-                double s = 0.0;
-                for (int k = i; k < j; ++k) s += X[i * MH + k] * U[k * d + j];
-                x = -s / U[j * d + j];
-            }
-            X[i * MH + j] = x;
-        }
-        __syncwarp();
-    }
-    double f1 = 0.0, f2 = 0.0;
-    for (int e = lane; e < d * d; e += 32) {
-        int i = e / d, j = e % d;
-        if (j < i) continue;
-        f1 += U[e] * U[e];
-        f2 += X[i * MH + j] * X[i * MH + j];
-    }
-    f1 = warp_sum(f1);
-    f2 = warp_sum(f2);
-    const double u = 0x1p-53, gam = (d + 1) * u / (1.0 - (d + 1) * u);
-    const double K = 2.0 * f1 * f2;              // 2x for the rounding in computing f2
-    if (!(gam * K <= 1e-3))                  // ill-conditioned: maybe not positive definite
-        return witness_not_pd(MAT, d, U, W->X, lane) ? ST_NOT_PD : ST_PRECISION;
-    const double slack_chol = 2.0 * gam * K * ((double)g.qmax + 1.0);
-    float *U32 = (float *)(slab + L.u32);
-    double *UI = (double *)(slab + L.ui64);
-    float *UI32 = (float *)(slab + L.ui32);
-    for (int e = lane; e < d * d; e += 32) U32[e] = (float)U[e];
-    __syncwarp();
-    for (int i = lane; i < d; i += 32) { UI[i] = 1.0 / U[i * d + i]; UI32[i] = 1.0f / U32[i * d + i]; }
-    // Tree estimate (Gaussian heuristic): the points of the projected lattice
-    // of the last k coordinates inside the ellipsoid's shadow, summed over k.
-    // The GCD rows below only prune, so a direction whose tree is small
-    // (or whose root interval is empty) is searched without them: building
-    // them costs more than they could save there.
-    bool want_rows = A.gcd_min_tree <= 0.0;
-    if (!want_rows) {
-        double est = 0.0;
-        if (lane == 0) {
-            const double lq = log((double)g.qmax + 1.0) + 1.1447298858494002;   // + log(pi)
-            double ldet = 0.0;
-            for (int k = 1; k <= d; ++k) {
-                ldet += log(U[(d - k) * d + (d - k)]);
-                est += exp(0.5 * k * lq - lgamma(0.5 * k + 1.0) - ldet);
-            }
-            if (m0_level == d - 1 && g.linmin > 0) {          // root interval under the M0 cut
-                const double rmax = sqrt((double)g.qmax + slack_chol + 1.0) / U[(d - 1) * d + (d - 1)];
-                const double cmin = ceil((double)g.linmin / fabs((double)g_lin));
-                if (cmin > rmax * (1.0 + 1e-9) + 1e-9) est = 0.0;
-            }
-        }
-        est = __shfl_sync(FULL, est, 0);
-        want_rows = est >= A.gcd_min_tree;
-    }
     int64_t *H = slab + L.H;
     for (int e = lane; e < d * d; e += 32) H[e] = 0;
     uint64_t hrows = 0;
@@ -1113,12 +1040,125 @@ h_done:
     return ST_PENDING;
 }
 
+// Phase 3 (split form): the GCD rows and bounds of a direction phase 2 queued.
+template <int N> __device__ int setup_phase3(const SetupArgs &A, int pid, int lane, int &stage, LllMem<N> *S)
+{
+    return setup_rows_bounds<N>(A, pid, lane, stage, S, true, A.dirs[pid].slack_chol);
+}
+
+template <int N> __device__ int setup_phase2(const SetupArgs &A, int pid, int lane, int &stage, LllMem<N> *S)
+{
+    SetupScratch *W = A.scratch + (blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5));
+    const Geo g = A.geo[A.pgeo[pid]];
+    const int h = g.h, d = h - 1;
+    int64_t *slab = A.slab + A.slab_off[pid];
+    const Slab L = slab_layout(h, d);
+    Dir &D = A.dirs[pid];
+    StageClock clk(stage, lane);
+    int64_t *MAT = slab + L.mat;
+    const int m0_level = D.m0_level;
+    const int64_t g_lin = D.g_lin;
+    clk.mark(10);
+    // 10. FP64 Cholesky of mat, certificate, float copies
+    double *U = (double *)(slab + L.u64);
+    for (int e = lane; e < d * d; e += 32) U[e] = 0.0;
+    __syncwarp();
+    bool notpd = false;
+    for (int j = 0; j < d; ++j) {
+        // row j of U: U_jj = sqrt(A_jj - sum_{k<j} U_kj^2), U_ji = (A_ji - sum_k U_kj U_ki) / U_jj
+        double s0 = 0.0;
+        for (int k = 0; k < j; ++k) { double u = U[k * d + j]; s0 += u * u; }
+        double pj = (double)MAT[j * d + j] - s0;
+        if (!(pj > 0)) { notpd = true; break; }
+        double ujj = sqrt(pj);
+        for (int i = j + 1 + lane; i < d; i += 32) {
+            double s = 0.0;
+            for (int k = 0; k < j; ++k) s += U[k * d + j] * U[k * d + i];
+            U[j * d + i] = ((double)MAT[j * d + i] - s) / ujj;
+        }
+        if (lane == 0) U[j * d + j] = ujj;
+        __syncwarp();
+    }
+    if (notpd)                               // not positive definite, or not decided here
+        return witness_not_pd(MAT, d, U, W->X, lane) ? ST_NOT_PD : ST_PRECISION;
+    // ||U||_F^2 and ||U^-1||_F^2
+    double *X = W->X;
+    for (int j = 0; j < d; ++j) {
+        for (int i = lane; i <= j; i += 32) {
+            double x;
+            if (i == j) x = 1.0 / U[j * d + j];
+            else {
+                double s = 0.0;
+                for (int k = i; k < j; ++k) s += X[i * MH + k] * U[k * d + j];
+                x = -s / U[j * d + j];
+            }
+            X[i * MH + j] = x;
+        }
+        __syncwarp();
+    }
+    double f1 = 0.0, f2 = 0.0;
+    for (int e = lane; e < d * d; e += 32) {
+        int i = e / d, j = e % d;
+        if (j < i) continue;
+        f1 += U[e] * U[e];
+        f2 += X[i * MH + j] * X[i * MH + j];
+    }
+    f1 = warp_sum(f1);
+    f2 = warp_sum(f2);
+    const double u = 0x1p-53, gam = (d + 1) * u / (1.0 - (d + 1) * u);
+    const double K = 2.0 * f1 * f2;              // 2x for the rounding in computing f2
+    if (!(gam * K <= 1e-3))                  // ill-conditioned: maybe not positive definite
+        return witness_not_pd(MAT, d, U, W->X, lane) ? ST_NOT_PD : ST_PRECISION;
+    const double slack_chol = 2.0 * gam * K * ((double)g.qmax + 1.0);
+    float *U32 = (float *)(slab + L.u32);
+    double *UI = (double *)(slab + L.ui64);
+    float *UI32 = (float *)(slab + L.ui32);
+    for (int e = lane; e < d * d; e += 32) U32[e] = (float)U[e];
+    __syncwarp();
+    for (int i = lane; i < d; i += 32) { UI[i] = 1.0 / U[i * d + i]; UI32[i] = 1.0f / U32[i * d + i]; }
+    // Tree estimate (Gaussian heuristic): the points of the projected lattice
+    // of the last k coordinates inside the ellipsoid's shadow, summed over k.
+    // The GCD rows below only prune, so a direction whose tree is small
+    // (or whose root interval is empty) is searched without them: building
+    // them costs more than they could save there.
+    bool want_rows = A.gcd_min_tree <= 0.0;
+    if (!want_rows) {
+        double est = 0.0;
+        if (lane == 0) {
+            const double lq = log((double)g.qmax + 1.0) + 1.1447298858494002;   // + log(pi)
+            double ldet = 0.0;
+            for (int k = 1; k <= d; ++k) {
+                ldet += log(U[(d - k) * d + (d - k)]);
+                est += exp(0.5 * k * lq - lgamma(0.5 * k + 1.0) - ldet);
+            }
+            if (m0_level == d - 1 && g.linmin > 0) {          // root interval under the M0 cut
+                const double rmax = sqrt((double)g.qmax + slack_chol + 1.0) / U[(d - 1) * d + (d - 1)];
+                const double cmin = ceil((double)g.linmin / fabs((double)g_lin));
+                if (cmin > rmax * (1.0 + 1e-9) + 1e-9) est = 0.0;
+            }
+        }
+        est = __shfl_sync(FULL, est, 0);
+        want_rows = est >= A.gcd_min_tree;
+    }
+    if (want_rows && A.rows_list) {
+        // (split form) the GCD rows are built by phase 3, over the directions that want them
+        if (lane == 0) {
+            D.slack_chol = slack_chol;
+            A.rows_list[atomicAdd(A.rows_count, 1u)] = pid;
+        }
+        __syncwarp();
+        return ST_WANT_ROWS;
+    }
+    return setup_rows_bounds<N>(A, pid, lane, stage, S, want_rows, slack_chol);
+}
+
 template <int N, int PH> __device__ __forceinline__ int setup_phase(const SetupArgs &A, int pid, int lane, int &stage,
                                                                    LllMem<N> *S)
 {
     if (PH == 0) return setup_phase0<N>(A, pid, lane, stage, S);
     if (PH == 1) return setup_phase1<N>(A, pid, lane, stage, S);
-    return setup_phase2<N>(A, pid, lane, stage, S);
+    if (PH == 2) return setup_phase2<N>(A, pid, lane, stage, S);
+    return setup_phase3<N>(A, pid, lane, stage, S);
 }
 
 // All three phases of one direction in sequence (the no-allocation entry point).
@@ -1145,11 +1185,12 @@ template <int N, int PH> __global__ void __launch_bounds__(128) k_setup(SetupArg
     const int lane = threadIdx.x & 31;
     SetupScratch *Wg = A.scratch + (blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5));
     LllMem<N> *S = A.smem_core ? (LllMem<N> *)smem_raw + (threadIdx.x >> 5) : (LllMem<N> *)&Wg->core;
+    const unsigned n = A.n_dev ? *A.n_dev : (unsigned)A.n;
     for (;;) {
         unsigned t = 0;
         if (lane == 0) t = atomicAdd(A.next, 1u);
         t = __shfl_sync(FULL, t, 0);
-        if (t >= (unsigned)A.n) break;
+        if (t >= n) break;
         const int pid = A.todo ? A.todo[t] : (int)t;
         const Geo g = A.geo[A.pgeo[pid]];
         if (PH == 0) {
@@ -1158,7 +1199,7 @@ template <int N, int PH> __global__ void __launch_bounds__(128) k_setup(SetupArg
                 D.geo = A.pgeo[pid]; D.h = g.h; D.d = g.h - 1; D.slab = A.slab_off[pid];
                 D.m0_level = -1; D.g_lin = 0; D.hrows = 0; D.slack_chol = 0.0;
             }
-        } else if (A.dirs[pid].status != ST_PENDING) {
+        } else if (A.dirs[pid].status != (PH == 3 ? ST_WANT_ROWS : ST_PENDING)) {
             continue;
         }
         __syncwarp();

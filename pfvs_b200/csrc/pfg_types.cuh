@@ -19,6 +19,7 @@ enum : int {
     ST_OK = 0,          // searched, points emitted
     ST_EMPTY = 3,       // M0 == 0 on the whole lattice and M0min > 0: no points
     ST_PENDING = 4,     // set up, not searched yet
+    ST_WANT_ROWS = 5,   // (internal) set up but for its GCD rows: queued for setup phase 3
     ST_RANGE = -8,      // a coordinate range exceeds int32 (reference status -8)
     ST_NOT_PD = -9,     // ellipsoid matrix not positive definite (reference -9)
     ST_FLOAT = -11,     // FP32 error bound exceeded: search again in FP64

@@ -83,6 +83,11 @@ extern "C" int emu_coni_batch(const pfg_input *in, int precision, int n_warps, p
                  dirs.data(), scratch.data(), (int)o32.size(), &next, o32.data(), 0, g_emu_gcd_min_tree};
     SetupArgs SA64 = SA;
     SA64.n = (int)o64.size(); SA64.next = &next64; SA64.todo = o64.data();
+    // the library's split form: phase 2 queues the directions that want GCD rows
+    std::vector<int32_t> rows32(nb + 1), rows64(nb + 1);
+    unsigned nrows32 = 0, nrows64 = 0;
+    SA.rows_list = rows32.data(); SA.rows_count = &nrows32;
+    SA64.rows_list = rows64.data(); SA64.rows_count = &nrows64;
     fprintf(stderr, "emu: setup\n");
     // the three phase kernels in order, each with a fresh work counter
     if (!o32.empty()) launch(setup_warps, [&] { k_setup<32, 0>(SA); });
@@ -93,7 +98,12 @@ extern "C" int emu_coni_batch(const pfg_input *in, int precision, int n_warps, p
     next = 0; next64 = 0;
     if (!o32.empty()) launch(setup_warps, [&] { k_setup<32, 2>(SA); });
     if (!o64.empty()) launch(setup_warps, [&] { k_setup<MH, 2>(SA64); });
-    fprintf(stderr, "emu: setup done\n");
+    next = 0; next64 = 0;
+    SA.todo = rows32.data(); SA.n_dev = &nrows32;
+    SA64.todo = rows64.data(); SA64.n_dev = &nrows64;
+    if (!o32.empty()) launch(setup_warps, [&] { k_setup<32, 3>(SA); });
+    if (!o64.empty()) launch(setup_warps, [&] { k_setup<MH, 3>(SA64); });
+    fprintf(stderr, "emu: setup done (%u + %u directions with GCD rows)\n", nrows32, nrows64);
 
     const unsigned long long pts_cap = 1 << 20;
     const unsigned q_cap = 1 << 14;
