@@ -515,6 +515,27 @@ def main():
                                              "fraction of the FP32 test's safety margin, interval endpoints "
                                              "(coordinate units, including the FP32 margin's widening), and levels "
                                              "whose FP32 range misses part of the FP64 one")
+    # the reference's own CUDA backend (oracle/_refgpu, its PFL_MAX_H11 = 24 build, in a process
+    # of its own) on the batch's h11 <= 24 directions, beside this library on the same directions
+    ref_gpu = None
+    if rank == 0 and world == 1 and not args.no_extras:
+        from oracle import refgpu
+        keep_g = [k for k, g in enumerate(geoms) if np.asarray(g["kappa"]).shape[0] <= 24]
+        if refgpu.available(24) and keep_g:
+            remap = {k: i for i, k in enumerate(keep_g)}
+            sel = np.flatnonzero(np.isin(pgeo, keep_g))
+            g24 = [geoms[k] for k in keep_g]
+            p24 = ps[sel]
+            pg24 = np.array([remap[int(x)] for x in pgeo[sel]], dtype=np.int32)
+            rr = refgpu.coni_batch_multi(g24, list(p24), pg24, max_h11=24, reps=3)
+            ours = [gpu.coni_batch_multi_ex(g24, p24, pg24, device=device, **tuned) for _ in range(3)][1:]
+            ref_gpu = {"directions": int(len(sel)), "reference_finished": float(np.mean(rr[4] == 0)),
+                       "reference_device_ms": rr[5] * 1e3, "reference_wall_ms": rr[6] * 1e3,
+                       "ours_device_ms": float(np.mean([o[5] for o in ours])) * 1e3,
+                       "what": "pfvs/fp_kernel/cuda/pfvs_gpu.cu built for sm_100a (PFL_MAX_H11 = 24), the same "
+                               "directions; it hands the directions it does not finish (pstat 1) to the CPU, "
+                               "whose time is not in its figure"}
+            ref_gpu["ours_vs_reference_device"] = ref_gpu["reference_device_ms"] / ref_gpu["ours_device_ms"]
     # PFVs: the batch through the device post-processing (pfg_coni_pfvs), once,
     # untimed, and PFVs/s on the reference's dataset geometries (which have PFVs)
     pfv = None
@@ -577,7 +598,7 @@ def main():
                              "output": per_step["ms_output"]},
                 "timed_form_nodes_per_step": int(per_step["nodes"]), "wall_ms_per_step": wall_s / args.steps * 1e3,
                 "clocks": clk_sum, "e2e": e2e, "cpu_baseline": cpu, "roofline": roofline,
-                "roofline_setup": roofline_setup, "forms": forms, "pfvs": pfv,
+                "roofline_setup": roofline_setup, "forms": forms, "pfvs": pfv, "ref_gpu": ref_gpu,
                 "gpu_launches": int(tot["launches"])}
         print(json.dumps(line))
     if pg is not None:
