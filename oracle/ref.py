@@ -60,6 +60,8 @@ def _load():
             ctypes.POINTER(_i32p), ctypes.POINTER(_i64p), ctypes.POINTER(ctypes.c_long),
             ctypes.POINTER(ctypes.c_long)]
         lib.ref_free.argtypes = [ctypes.c_void_p]
+        lib.ref_coni_mu0.restype = ctypes.c_int
+        lib.ref_coni_mu0.argtypes = [ctypes.c_int, _i64p, _i64p, _i64p, _i64p, _i64p]
         lib.ref_lattice_build.restype = ctypes.c_int
         lib.ref_lattice_build.argtypes = [
             ctypes.c_int, _i64p, _i64p, _i64p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
@@ -204,3 +206,17 @@ def lattice_build(kappa, Mbasis, p, coni=True, extra_lll=True, m0_basis=True):
                 row.append((hi << 64) + lo)
             H.append(row)
     return (st, Z.reshape(h, h), B.reshape(h, d), ZB.reshape(h, d), mat.reshape(d, d), H)
+
+
+def coni_mu0(kappa, p_r):
+    """The reference's C dilation bound (coni_bound.h:255): (status, mu0 as a
+    Fraction or None, K) with status 0 decided, 1 no bound, < 0 undecided in C."""
+    from fractions import Fraction
+    lib = _load()
+    kappa = np.ascontiguousarray(kappa, dtype=np.int64)
+    h = kappa.shape[0]
+    p_r = np.ascontiguousarray(p_r, dtype=np.int64).reshape(h - 1)
+    num, den = np.zeros(1, np.int64), np.zeros(1, np.int64)
+    K = np.zeros(h - 1, np.int64)
+    st = lib.ref_coni_mu0(h, _p(kappa), _p(p_r), _p(num), _p(den), _p(K))
+    return st, (Fraction(int(num[0]), int(den[0])) if st == 0 else None), K

@@ -285,3 +285,14 @@ int ref_lattice_build(int h, const int64_t *kappa, const int64_t *Mbasis,
     free(R);
     return st;
 }
+
+/* The reference's coni dilation bound mu0 (pfvs/fp_kernel/coni_bound.h:255,
+ * the C path of pfvs.dilation.coni_mu0, dilation.py:145): status 0 with
+ * mu0 = *num / *den and K a minimizer (h - 1 entries), 1 when the bound's
+ * hypotheses fail (A_rr singular, s > 0, S not positive definite on Lambda),
+ * < 0 when the C path cannot decide (the reference then uses flint). */
+#include "coni_bound.h"
+int ref_coni_mu0(int h, const int64_t *kappa, const int64_t *p_r, int64_t *num, int64_t *den, int64_t *K)
+{
+    return cb_coni_mu0(h, kappa, p_r, num, den, K);
+}
