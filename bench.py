@@ -382,12 +382,12 @@ def main():
         lo, hi = bounds[k]
         return gpu.coni_batch_multi_ex(geoms, ps[lo:hi], pgeo[lo:hi], device=device, **kw)
 
-    # the search grid and GCD-row policy from the autotuner (tuned on a sample of
-    # the batch, or read from its JSON store), untimed; they change time only
+    # the search grid and GCD-row policy from the autotuner (tuned on the batch, or
+    # read from its JSON store), untimed; they change time only
     tuned = {}
     if not args.no_tune and args.form == "batched":
         from pfvs_b200 import tune
-        tuned = tune.autotune(geoms, ps, pgeo, device=device, n_sample=8192)
+        tuned = tune.autotune(geoms, ps, pgeo, device=device)
 
     # work unit: nodes of the FP64-pruned tree with every GCD-cut row built (the
     # reference's pruning), counted once, untimed; the timed steps build the

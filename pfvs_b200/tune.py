@@ -11,8 +11,11 @@ are split dynamically by donation, so the grid and the row policy are what
 is left to choose.  None of them changes the points (only time and node
 counts), so a tuned call returns the same arrays as an untuned one.
 
-The tuner times candidate settings on a stratified sample of the batch (the
-library's own device time of setup + search, best of `reps`), by
+The tuner times candidate settings on the batch itself, or on a stratified
+sample of it (the library's own device time of setup + search, best of
+`reps`); a sample much smaller than the batch can mislead it (on 8,192 of the
+mixed batch's 65,536 directions it preferred a smaller grid that ran the full
+batch's search 38 % slower), so the default is the whole batch, by
 coordinate descent: the row policy first, then the block shape, then the
 grid.  Results are kept per (device name, batch class) in a JSON file
 (default ~/.cache/pfvs_b200/tune.json, or PFVS_B200_TUNE), where the batch
@@ -113,30 +116,32 @@ def search(run, candidates=None):
     return best, best_ms, trials
 
 
-def autotune(geoms, ps, pgeo, device=0, n_sample=8192, reps=2, path=None, retune=False, run=None):
+def autotune(geoms, ps, pgeo, device=0, n_sample=None, reps=2, path=None, retune=False, run=None):
     """
     Options for coni_batch_multi_ex tuned for this batch's class on this
     device: a stored result when there is one (unless retune), else a
-    coordinate-descent search on a stratified sample of the batch, stored.
+    coordinate-descent search on the batch (or a stratified sample of
+    n_sample directions), stored.
     `run` (opts -> ms) replaces the device timing (tests).
     """
     key_dev = "cpu"
     if run is None:
-        from . import gpu
         try:
             import torch
             key_dev = torch.cuda.get_device_name(device).replace(" ", "_")
         except Exception:
             key_dev = f"device{device}"
-        idx = sample(pgeo, n_sample)
-        sps = [ps[i] for i in idx]
-        spgeo = np.asarray(pgeo)[idx]
-        gpu.coni_batch_multi_ex(geoms, sps, spgeo, device=device)      # (warm: buffers, module)
-        run = _device_time(geoms, sps, spgeo, device, reps)
     key = f"{key_dev}|{batch_class(geoms)}"
     table = load(path)
     if key in table and not retune:
         return dict(table[key]["options"])
+    if run is None:
+        from . import gpu
+        idx = sample(pgeo, n_sample or len(pgeo))
+        sps = ps[idx] if isinstance(ps, np.ndarray) else [ps[i] for i in idx]
+        spgeo = np.asarray(pgeo)[idx]
+        gpu.coni_batch_multi_ex(geoms, sps, spgeo, device=device)      # (warm: buffers, module)
+        run = _device_time(geoms, sps, spgeo, device, reps)
     best, best_ms, trials = search(run)
     table[key] = {"options": best, "ms": best_ms, "default_ms": trials[json.dumps(DEFAULTS, sort_keys=True)],
                   "trials": len(trials)}
