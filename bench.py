@@ -353,6 +353,92 @@ def pfv_rates(gpu, device, threads):
     return out
 
 
+def coni_zp_rates(device, threads):
+    """The exhaustive coniZp driver (pfvs_b200.coni: the dilation bound of
+    every direction on the device, then coniZpM at each direction's grid_up
+    bound with the device post-processing) on the dataset geometries, against
+    the same plan on the host: the reference's C bound (coni_bound.h:255),
+    the reference kernel at the same dilations and the oracle's restated
+    post-processing, on `threads` threads.  And the bound alone at volume:
+    directions/s of k_mu0 against the reference's C bound on a batch of
+    the mixed workload's h11 = 8 and 16 directions."""
+    import concurrent.futures as cf
+    from oracle import postproc, ref
+    from pfvs_b200 import coni, dilation, workloads
+    G = np.load(os.path.join(ROOT, "tests", "golden", "dataset_pfvs.npz"))
+    data = []
+    for k in range(int(G["n_geometries"][0])):
+        h, Q, m0 = (int(x) for x in G[f"g{k}_scal"])
+        data.append(dict(kappa=G[f"g{k}_kappa"], Mbasis=G[f"g{k}_Mbasis"], Q=Q, M0min=m0, ps=G[f"g{k}_ps"][:, 1:]))
+    n_dirs = sum(len(g["ps"]) for g in data)
+
+    def device_run():
+        t0 = time.perf_counter()
+        n_pfv, t_b, dil_max = 0, 0.0, 0
+        for g in data:
+            Ks, Ms, complete, info = coni.coni_zp(g["kappa"], g["Mbasis"], g["ps"], g["Q"], M0min=g["M0min"],
+                                                  device=device, return_info=True)
+            n_pfv += len(Ks)
+            t_b += info["seconds_bound"]
+            dil_max = max(dil_max, int(info["dilation"].max()))
+        return time.perf_counter() - t0, t_b, n_pfv, dil_max
+    device_run()                                                    # (warm)
+    runs = [device_run() for _ in range(3)]
+    best = min(runs)
+    out = {"workload": f"{len(data)} reference dataset geometries (h11 3..9), {n_dirs} p-vectors, every PFV of "
+                       f"each direction at any dilation (searched to grid_up(ceil(Q / mu0)), up to {best[3]})",
+           "pfvs": int(best[2]), "wall_s": best[0], "bound_wall_s": best[1], "pfvs_per_s": best[2] / best[0],
+           "directions_per_s": n_dirs / best[0]}
+    if ref.available():
+        def host_one(g):
+            st, num, den, _ = ref.coni_mu0_batch(g["kappa"], g["ps"])
+            bc, fits = dilation._ceil_q_over(g["Q"], num[st == 0], den[st == 0])
+            b = np.zeros(len(st), np.int64)
+            b[st == 0] = bc
+            dil = coni.route(b, 1)
+            h = g["kappa"].shape[0]
+            P = np.hstack([np.zeros((len(g["ps"]), 1), np.int64), g["ps"]])
+            n = 0
+            for D in np.unique(dil):
+                sel = np.flatnonzero(dil == D)
+                M_, Kn_, q_, pl, stt, _ = ref.coni_batch(g["kappa"], g["Mbasis"], P[sel], g["Q"], float(D), g["M0min"])
+                eK, eM, ek = postproc.pfvs_from_points(M_, Kn_, q_, pl, g["kappa"], h, g["Q"], g["M0min"])
+                n += len(ek)
+            return n
+        t0 = time.perf_counter()
+        with cf.ThreadPoolExecutor(threads) as ex:
+            n_host = sum(ex.map(host_one, sorted(data, key=lambda g: -len(g["ps"]) * g["kappa"].shape[0] ** 3)))
+        dt = time.perf_counter() - t0
+        out["cpu_reference"] = {"pfvs": int(n_host), "wall_s": dt, "pfvs_per_s": n_host / dt, "threads": threads,
+                                "what": "oracle/_ref: the reference's C bound + its kernel at the same dilations "
+                                        "+ the oracle's restated post-processing"}
+        out["device_vs_cpu_reference"] = dt / best[0]
+    # the bound at volume
+    w = workloads.build("mixed", n_p=16384)
+    vol = {}
+    for k, g in enumerate(w.geoms):
+        if g.h11 not in (8, 16) or g.h11 in vol:
+            continue
+        P = np.array([w.ps[i][1:] for i in np.flatnonzero(np.asarray(w.pgeo) == k)])
+        dilation.coni_mu0_batch(P[:256], g.kappa, device=device)    # (warm)
+        t0 = time.perf_counter()
+        st, *_ = dilation.coni_mu0_batch(P, g.kappa, device=device)
+        dt = time.perf_counter() - t0
+        ent = {"directions": int(len(P)), "device_directions_per_s": len(P) / dt,
+               "device_decided": float(np.mean(st >= 0))}
+        if ref.available():
+            t1 = time.perf_counter()
+            with cf.ThreadPoolExecutor(threads) as ex:
+                parts = list(ex.map(lambda c: ref.coni_mu0_batch(g.kappa, c), np.array_split(P, 4 * threads)))
+            dr = time.perf_counter() - t1
+            sr = np.concatenate([x[0] for x in parts])
+            ent.update({"cpu_reference_directions_per_s": len(P) / dr, "cpu_reference_decided": float(np.mean(sr >= 0)),
+                        "threads": threads})
+        vol[f"h11={g.h11}"] = ent
+    out["bound_at_volume"] = vol
+    return out
+
+
 def main():
     args = parse()
     world, rank, local, pg = dist_init()
@@ -550,6 +636,7 @@ def main():
                "device_ms": allmax(pg, sum(x[2] for x in pr)) * 1e3}
         if rank == 0 and world == 1:
             pfv["dataset"] = pfv_rates(gpu, device, threads)
+            pfv["coni_zp"] = coni_zp_rates(device, threads)
     # roofline of the search kernel: executed warp instructions per launch (ncu
     # per-node figure x the launch's nodes) over its CUDA-event time (the
     # search stage: k_flip, a few microseconds, then k_search<double, 1>); the

@@ -161,6 +161,21 @@ int pfg_coni_pfvs(const pfg_input *in, const pfg_options *opt, pfg_pfv_output *o
 /* Free a pfg_pfv_output's arrays (safe on a zeroed struct). */
 void pfg_pfv_output_free(pfg_pfv_output *out);
 
+/* The coni dilation bound of n_p directions p_hat = (0, p_r) of one geometry
+ * (kappa, h^3): mu0 = min over nonzero K in Z^(h-1) with p_r . K = 0 of
+ * -K^T A_rr^-1 K, A = kappa . p_hat, so that every coni PFV with direction
+ * p_hat has dilation below Q / mu0 -- the reference's coni_mu0
+ * (pfvs/dilation.py:145, its C path pfvs/fp_kernel/coni_bound.h:255, called
+ * in batches by _coni_mu0_batch).  p_r: (n_p, h-1) row-major.  Per
+ * direction: status 0 with mu0 = mu_num / mu_den in lowest terms and K
+ * ((n_p, h-1)) a minimizer; 1 no bound (A_rr singular, s > 0, or the form
+ * not positive definite on the lattice); < 0 not decided on the device (an
+ * exact value beyond int128, an ill-conditioned form, the search's node
+ * budget).  3 <= h <= 32.  Returns 0, or 1 with err (256 chars, may be NULL)
+ * set. */
+int pfg_coni_mu0_batch(int h, const int64_t *kappa, int64_t n_p, const int64_t *p_r, int device,
+                       int32_t *status, int64_t *mu_num, int64_t *mu_den, int64_t *K, char *err);
+
 /* Test hook (no counterpart in the reference): the k-th device allocation
  * this library makes from now on (k >= 1) fails once with
  * cudaErrorMemoryAllocation, without allocating, so that tests can drive the

@@ -62,6 +62,9 @@ def _load():
         lib.ref_free.argtypes = [ctypes.c_void_p]
         lib.ref_coni_mu0.restype = ctypes.c_int
         lib.ref_coni_mu0.argtypes = [ctypes.c_int, _i64p, _i64p, _i64p, _i64p, _i64p]
+        lib.ref_coni_mu0_batch.restype = None
+        lib.ref_coni_mu0_batch.argtypes = [ctypes.c_int, _i64p, ctypes.c_int64, _i64p,
+                                           ctypes.POINTER(ctypes.c_int32), _i64p, _i64p, _i64p]
         lib.ref_lattice_build.restype = ctypes.c_int
         lib.ref_lattice_build.argtypes = [
             ctypes.c_int, _i64p, _i64p, _i64p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
@@ -220,3 +223,19 @@ def coni_mu0(kappa, p_r):
     K = np.zeros(h - 1, np.int64)
     st = lib.ref_coni_mu0(h, _p(kappa), _p(p_r), _p(num), _p(den), _p(K))
     return st, (Fraction(int(num[0]), int(den[0])) if st == 0 else None), K
+
+
+def coni_mu0_batch(kappa, P):
+    """The reference's C dilation bound over the rows of P ((n, h-1)), in one
+    C loop: (status int32, mu_num, mu_den, K) arrays."""
+    lib = _load()
+    kappa = np.ascontiguousarray(kappa, dtype=np.int64)
+    h = kappa.shape[0]
+    P = np.ascontiguousarray(np.atleast_2d(P), dtype=np.int64).reshape(-1, h - 1)
+    n = len(P)
+    st = np.zeros(max(n, 1), np.int32)
+    num, den = np.zeros(max(n, 1), np.int64), np.zeros(max(n, 1), np.int64)
+    K = np.zeros((max(n, 1), h - 1), np.int64)
+    lib.ref_coni_mu0_batch(h, _p(kappa), n, _p(P), st.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)), _p(num),
+                           _p(den), _p(K))
+    return st[:n], num[:n], den[:n], K[:n]

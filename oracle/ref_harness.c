@@ -296,3 +296,11 @@ int ref_coni_mu0(int h, const int64_t *kappa, const int64_t *p_r, int64_t *num, 
 {
     return cb_coni_mu0(h, kappa, p_r, num, den, K);
 }
+
+/* the same over the n rows of P ((n, h-1)): statuses into st */
+void ref_coni_mu0_batch(int h, const int64_t *kappa, int64_t n, const int64_t *P, int32_t *st, int64_t *num,
+                        int64_t *den, int64_t *K)
+{
+    for (int64_t i = 0; i < n; ++i)
+        st[i] = cb_coni_mu0(h, kappa, P + i * (h - 1), num + i, den + i, K + i * (h - 1));
+}

@@ -32,6 +32,7 @@
 #include "pfg_search.cuh"
 #include "pfg_out.cuh"
 #include "pfg_pfv.cuh"
+#include "pfg_mu0.cuh"
 
 using namespace pfg;
 
@@ -61,7 +62,7 @@ enum {
     W_CTL, W_ITEMS, W_READY, W_HDR, W_COORDS, W_DIRNODES, W_DIRPASS,
     W_KEYS, W_COUNT, W_FILL, W_SEG, W_IDX, W_CSEG, W_SUM, W_PERM, W_PERM2, W_SIDX, W_PCNT, W_PKG, W_PEPT, W_PEG, W_PEK0, W_PEORD, W_PNONS, W_PKEEP,
     W_PERR, W_PSORT, W_PK, W_PM, W_PP, W_PRIMES, W_OM, W_OK, W_OQ, W_OP, W_OM2, W_OK2, W_OQ2, W_OP2, W_RETRY,
-    W_ROWS, W_N
+    W_ROWS, W_MU_K, W_MU_P, W_MU_ST, W_MU_NUM, W_MU_DEN, W_MU_KO, W_MU_SCR, W_MU_CTR, W_N
 };
 
 struct Workspace {
@@ -946,4 +947,59 @@ extern "C" void pfg_pfv_output_free(pfg_pfv_output *out)
     out->K = out->M = out->pidx = nullptr;
     out->pstat = nullptr;
     out->n = 0;
+}
+
+// The coni dilation bound mu0 of n_p directions of one geometry (pfg_mu0.cuh).
+extern "C" int pfg_coni_mu0_batch(int h, const int64_t *kappa, int64_t n_p, const int64_t *p_r, int device,
+                                  int32_t *status, int64_t *mu_num, int64_t *mu_den, int64_t *K, char *err)
+{
+    char msg[256] = "";
+    int rc = 0;
+    if (h < 3 || h > MU0_MAXH || n_p < 0 || n_p > INT32_MAX || (n_p && (!kappa || !p_r || !status || !mu_num ||
+                                                                        !mu_den || !K))) {
+        snprintf(msg, sizeof msg, "pfg_coni_mu0_batch: bad arguments (h11 = %d outside 3..%d, or null arrays)",
+                 h, MU0_MAXH);
+        if (err) memcpy(err, msg, sizeof msg);
+        return 1;
+    }
+    if (n_p == 0) return 0;
+    const int m = h - 1;
+    Workspace &W = workspace(device);
+    std::lock_guard<std::mutex> lock(W.mu);
+    int64_t *dk, *dp, *dn, *dd, *dK; int32_t *ds; Mu0Scratch *dscr; unsigned *dctr;
+    int bps = 0, nsm = 148, grid = 0;
+    cudaError_t e;
+#define MCK(x) do { e = (x); if (e != cudaSuccess) { snprintf(msg, sizeof msg, "%s (%s:%d)", cudaGetErrorString(e), \
+    __FILE__, __LINE__); rc = 1; goto mu_fail; } } while (0)
+    MCK(cudaSetDevice(device));
+    MCK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device));
+    MCK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_mu0, 128, 0));
+    grid = (int)std::min<int64_t>((n_p + 3) / 4, (int64_t)nsm * std::max(1, bps));
+    MCK(ws_get(W, W_MU_K, (size_t)h * h * h * 8, (void **)&dk));
+    MCK(ws_get(W, W_MU_P, (size_t)n_p * m * 8, (void **)&dp));
+    MCK(ws_get(W, W_MU_ST, (size_t)n_p * 4, (void **)&ds));
+    MCK(ws_get(W, W_MU_NUM, (size_t)n_p * 8, (void **)&dn));
+    MCK(ws_get(W, W_MU_DEN, (size_t)n_p * 8, (void **)&dd));
+    MCK(ws_get(W, W_MU_KO, (size_t)n_p * m * 8, (void **)&dK));
+    MCK(ws_get(W, W_MU_SCR, (size_t)grid * 4 * sizeof(Mu0Scratch), (void **)&dscr));
+    MCK(ws_get(W, W_MU_CTR, 64, (void **)&dctr));
+    MCK(cudaMemcpy(dk, kappa, (size_t)h * h * h * 8, cudaMemcpyHostToDevice));
+    MCK(cudaMemcpy(dp, p_r, (size_t)n_p * m * 8, cudaMemcpyHostToDevice));
+    MCK(cudaMemset(dctr, 0, 64));
+    {
+        Mu0Args A{h, dk, dp, (int)n_p, dctr, dscr, ds, dn, dd, dK, 20000000ll};
+        k_mu0<<<grid, 128>>>(A);
+        MCK(cudaGetLastError());
+    }
+    MCK(cudaMemcpy(status, ds, (size_t)n_p * 4, cudaMemcpyDeviceToHost));
+    MCK(cudaMemcpy(mu_num, dn, (size_t)n_p * 8, cudaMemcpyDeviceToHost));
+    MCK(cudaMemcpy(mu_den, dd, (size_t)n_p * 8, cudaMemcpyDeviceToHost));
+    MCK(cudaMemcpy(K, dK, (size_t)n_p * m * 8, cudaMemcpyDeviceToHost));
+#undef MCK
+mu_fail:
+    if (rc) {
+        cudaGetLastError();
+        if (err) memcpy(err, msg, sizeof msg);
+    }
+    return rc;
 }

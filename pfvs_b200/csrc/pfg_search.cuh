@@ -252,24 +252,9 @@ template <class R> struct Lanes {
 #define LGET(S, f, i) shfl((NS > 1 && (i) >= 32) ? S.f##1 : S.f##0, (i) & 31)
 #define LSET(S, f, i, val) do { if (lane == ((i) & 31)) { if (NS > 1 && (i) >= 32) S.f##1 = (val); else S.f##0 = (val); } } while (0)
 
-// column i of H as the lanes' GCD-row prefixes need it when c[i] changes
-// (lane r: the entry of the row with pivot r; 0 where that row is not kept or
-// r >= i), loaded ahead of its use so that its latency hides behind the
-// candidate evaluation
-template <class R> struct HCol { int64_t h0, h1; };
-template <class R, int NS> __device__ __forceinline__ HCol<R> h_column(const Prob<R> &P, int i, int lane)
-{
-    HCol<R> c{0, 0};
-    const int d = P.d;
-    if (lane < i && ((P.hrows >> lane) & 1)) c.h0 = P.H[i * d + lane];
-    if (NS > 1 && lane + 32 < i && ((P.hrows >> (lane + 32)) & 1)) c.h1 = P.H[i * d + lane + 32];
-    return c;
-}
-
 // c[i] changes by dv (i >= 1): update the exact incremental sums (the GCD
-// rows' prefixes of the levels below i with column i of H, `hc`)
-template <class R, int NS> __device__ __forceinline__ void apply_dc(Lanes<R> &S, const Prob<R> &P, int i, int64_t dv,
-                                                                    const HCol<R> &hc, int lane)
+// rows' prefixes of the levels below i with column i of H)
+template <class R, int NS> __device__ __forceinline__ void apply_dc(Lanes<R> &S, const Prob<R> &P, int i, int64_t dv, int lane)
 {
     if (dv == 0 || i == 0) return;
     const int d = P.d, h = P.h;
@@ -277,8 +262,8 @@ template <class R, int NS> __device__ __forceinline__ void apply_dc(Lanes<R> &S,
     if (NS > 1 && lane + 32 < d) S.y1 += (int64_t)P.MAT[i * d + lane + 32] * dv;
     if (lane < h) S.k0 += (int64_t)P.ZT[i * h + lane] * dv;
     if (NS > 1 && lane + 32 < h) S.k1 += (int64_t)P.ZT[i * h + lane + 32] * dv;
-    S.hp0 += (i128)hc.h0 * dv;
-    if (NS > 1) S.hp1 += (i128)hc.h1 * dv;
+    if (lane < i && ((P.hrows >> lane) & 1)) S.hp0 += (i128)P.H[i * d + lane] * dv;
+    if (NS > 1 && lane + 32 < i && ((P.hrows >> (lane + 32)) & 1)) S.hp1 += (i128)P.H[i * d + lane + 32] * dv;
 }
 
 // the dot products of entering level i (c[i+1:] set): off, aoff, GCD prefix
@@ -492,7 +477,7 @@ __device__ int run_subtree(const SearchArgs &A, const Prob<R> &P, int pid, const
         // exact incremental sums from scratch
         for (int j = i + 1; j < d; ++j) {
             int32_t cj = shfl((NS > 1 && j >= 32) ? S.c1 : S.c0, j & 31);
-            apply_dc<R, NS>(S, P, j, cj, h_column<R, NS>(P, j, lane), lane);
+            apply_dc<R, NS>(S, P, j, cj, lane);
         }
         R off, aoff;
         i128 pre;
@@ -590,7 +575,6 @@ __device__ int run_subtree(const SearchArgs &A, const Prob<R> &P, int pid, const
         const i128 pre = u_pre;
         const bool hrow = (P.hrows >> i) & 1;
         const int64_t hii = P.HD[i];
-        const HCol<R> hcol = h_column<R, NS>(P, i, lane);     // (for a descent from this level)
         const R uii = P.U[upk(i, i, d)];
         const int64_t ncand = min((int64_t)32, hi - cur + 1);
         const int64_t v = cur + lane;
@@ -658,7 +642,7 @@ __device__ int run_subtree(const SearchArgs &A, const Prob<R> &P, int pid, const
             const R nr0 = shfl(nr, t0), en0 = shfl(en, t0);
             const u128 g0 = shflu128(gn, t0);
             const int32_t ci = LGET(S, c, i);
-            apply_dc<R, NS>(S, P, i, vc - ci, hcol, lane);
+            apply_dc<R, NS>(S, P, i, vc - ci, lane);
             LSET(S, c, i, (int32_t)vc);
             --i;
             u_rem = nr0; u_err = en0; u_gab = g0;

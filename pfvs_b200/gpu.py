@@ -115,6 +115,9 @@ def _load():
     lib.pfg_pfv_output_free.argtypes = [ctypes.POINTER(_PfvOutput)]
     lib.pfg_release.argtypes = [ctypes.c_int]
     lib.pfg_debug_fail_alloc.argtypes = [ctypes.c_int]
+    lib.pfg_coni_mu0_batch.argtypes = [ctypes.c_int, _i64p, ctypes.c_int64, _i64p, ctypes.c_int, _i32p,
+                                       _i64p, _i64p, _i64p, ctypes.c_char_p]
+    lib.pfg_coni_mu0_batch.restype = ctypes.c_int
     _lib = lib
     return lib
 

@@ -10,7 +10,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB = os.path.join(HERE, "_build", "libpfvs_emu.so")
 SRCS = [os.path.join(HERE, f) for f in ("emu_driver.cpp", "warp_emu.h")] + [
     os.path.join(HERE, "..", "..", "pfvs_b200", "csrc", f) for f in
-    ("pfg_int.cuh", "pfg_types.cuh", "pfg_setup.cuh", "pfg_search.cuh", "pfg_out.cuh")] + [
+    ("pfg_int.cuh", "pfg_types.cuh", "pfg_setup.cuh", "pfg_search.cuh", "pfg_out.cuh", "pfg_mu0.cuh")] + [
     os.path.join(HERE, "..", "..", "include", "pfvs_gpu.h")]
 _lib = None
 
@@ -96,3 +96,21 @@ def set_gcd_min_tree(v):
     """GCD-row policy of the emulated setup, as pfg_options.gcd_min_tree
     (0: the library default; < 0: rows for every direction)."""
     _load().emu_set_gcd_min_tree(float(v))
+
+
+def coni_mu0_batch(kappa, p_r):
+    """The device's coni dilation bound on the emulated warp: (status, mu_num,
+    mu_den, K) for the rows of p_r ((n, h-1))."""
+    lib = _load()
+    i64p, i32p = ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int32)
+    lib.emu_coni_mu0_batch.argtypes = [ctypes.c_int, i64p, ctypes.c_int64, i64p, i32p, i64p, i64p, i64p]
+    kappa = np.ascontiguousarray(kappa, dtype=np.int64)
+    h = kappa.shape[0]
+    p_r = np.ascontiguousarray(p_r, dtype=np.int64).reshape(-1, h - 1)
+    n = len(p_r)
+    st = np.zeros(max(n, 1), np.int32)
+    num, den = np.zeros(max(n, 1), np.int64), np.zeros(max(n, 1), np.int64)
+    K = np.zeros((max(n, 1), h - 1), np.int64)
+    lib.emu_coni_mu0_batch(h, kappa.ctypes.data_as(i64p), n, p_r.ctypes.data_as(i64p), st.ctypes.data_as(i32p),
+                           num.ctypes.data_as(i64p), den.ctypes.data_as(i64p), K.ctypes.data_as(i64p))
+    return st[:n], num[:n], den[:n], K[:n]

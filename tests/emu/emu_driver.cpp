@@ -20,6 +20,7 @@
 #include "../../pfvs_b200/csrc/pfg_setup.cuh"
 #include "../../pfvs_b200/csrc/pfg_search.cuh"
 #include "../../pfvs_b200/csrc/pfg_out.cuh"
+#include "../../pfvs_b200/csrc/pfg_mu0.cuh"
 
 using namespace pfg;
 
@@ -210,4 +211,16 @@ extern "C" int emu_witness_not_pd(const int64_t *A, int d)
         if ((threadIdx.x & 31) == 0) res = w ? 1 : 0;
     });
     return res;
+}
+
+
+// The device's coni dilation bound (pfg_mu0.cuh, k_mu0) on one emulated warp.
+extern "C" int emu_coni_mu0_batch(int h, const int64_t *kappa, int64_t n_p, const int64_t *p_r, int32_t *status,
+                                  int64_t *num, int64_t *den, int64_t *K)
+{
+    std::vector<Mu0Scratch> scr(1);
+    unsigned next = 0;
+    Mu0Args A{h, kappa, p_r, (int)n_p, &next, scr.data(), status, num, den, K, 20000000ll};
+    emu_run_warp(0, 0, 32, 1, [&] { k_mu0(A); });
+    return 0;
 }

@@ -79,10 +79,29 @@ def main():
     out = {k: np.array(v, dtype=np.int64) for k, v in rows.items()}
     for k, kap in enumerate(kappas):
         out[f"kappa{k}"] = kap
+    # directions that are not PFV directions (seeded, small entries), so that
+    # "no bound" (status 1) and undecided cases of the C code are covered too
+    rng = np.random.default_rng(7)
+    rnd = {"r_gidx": [], "r_p": [], "r_mu0": [], "r_status": []}
+    for k, kap in enumerate(kappas):
+        h = kap.shape[0]
+        for _ in range(12):
+            p_r = rng.integers(-3, 7, size=h - 1)
+            if not p_r.any():
+                continue
+            st, mu, _ = ref.coni_mu0(kap, p_r.astype(np.int64))
+            rnd["r_gidx"].append(k)
+            rnd["r_p"].append(list(p_r) + [0] * (64 - h))
+            rnd["r_mu0"].append((mu.numerator, mu.denominator) if st == 0 else (0, 0))
+            rnd["r_status"].append(st)
+    out.update({k: np.array(v, dtype=np.int64) for k, v in rnd.items()})
     np.savez_compressed(os.path.join(HERE, "mu0.npz"), **out)
     st = out["status"]
     print(f"{len(st)} PFVs over {len(kappas)} geometries; reference C decided {int(np.sum(st == 0))}, "
           f"no bound {int(np.sum(st == 1))}, undecided {int(np.sum(st < 0))}")
+    rs = out["r_status"]
+    print(f"{len(rs)} other directions; decided {int(np.sum(rs == 0))}, no bound {int(np.sum(rs == 1))}, "
+          f"undecided {int(np.sum(rs < 0))}")
 
 
 if __name__ == "__main__":

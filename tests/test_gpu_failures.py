@@ -33,13 +33,28 @@ def batch():
     return geoms, ps, pgeo, base
 
 
+@pytest.fixture(scope="module")
+def mixed_depths(batch):
+    """The mixed batch (small trees) with 32 directions of plain at dilation
+    3200 (trees of about a million nodes) appended, so that a short deadline
+    always cuts some directions and spares others."""
+    geoms, ps, pgeo, _ = batch
+    g2, p2, q2, _ = layout(workloads.build("plain", n_p=32, dilations=(3200.0,)))
+    geoms = list(geoms) + list(g2)
+    ps = list(ps) + list(p2)
+    pgeo = np.concatenate([pgeo, np.asarray(q2) + len(batch[0])]).astype(np.int32)
+    base = gpu.coni_batch_multi_ex(geoms, ps, pgeo)
+    assert np.all(base[4] == 0)
+    return geoms, ps, pgeo, base
+
+
 def _same_as_base(res, base):
     assert_same(res, base)
     np.testing.assert_array_equal(res[4], base[4])
 
 
-def test_deadline_marks_cut_directions_and_keeps_the_rest(batch):
-    geoms, ps, pgeo, base = batch
+def test_deadline_marks_cut_directions_and_keeps_the_rest(mixed_depths):
+    geoms, ps, pgeo, base = mixed_depths
     r = gpu.coni_batch_multi_ex(geoms, ps, pgeo, deadline_s=1e-6)
     cut = r[4] == -22
     assert cut.any() and not cut.all()
