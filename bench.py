@@ -442,6 +442,62 @@ def coni_zp_rates(device, threads):
     return out
 
 
+def nonconi_rates(device, threads):
+    """Non-coni ZpM (pfg_zpm_batch; the reference runs it on the CPU only) on
+    the reference's non-coni Manwe test geometry (tests/golden/nonconi.npz):
+    the 11,386 primitive p-vectors of the box |p| <= 6 in its Kahler cone at
+    dilation 3, Qmax = h11 + h21 + 2.  Device: setup + search time, nodes/s,
+    and PFVs/s through the product's host post-processing; against the
+    reference's C setup and kernel (oracle/_ref, composed as nonconi.ZpM
+    composes them) on `threads` threads."""
+    import concurrent.futures as cf
+    from oracle import nonconi as onc
+    from oracle import pvecs, ref
+    from pfvs_b200 import gpu, nonconi
+    G = np.load(os.path.join(ROOT, "tests", "golden", "nonconi.npz"))
+    kappa, Mb, H = G["c4_kappa"], G["c4_Mbasis"], G["c4_H"]
+    Qmin, Qmax = (int(x) for x in G["c4_scal"])
+    ps = np.array(pvecs.box_enum(6, H), dtype=np.int64)
+    geoms = [dict(kappa=kappa, Mbasis=Mb, Q=Qmax, dilation=3.0)]
+    pg = np.zeros(len(ps), np.int32)
+    gpu.zpm_batch_multi_ex(geoms, ps, pg, device=device)            # (warm)
+    runs = [gpu.zpm_batch_multi_ex(geoms, ps, pg, device=device) for _ in range(3)]
+    r = min(runs, key=lambda x: x[5])
+    st = r[6]
+    dev_s = (st["ms_setup"] + st["ms_search"] + st["ms_output"]) / 1e3
+    t0 = time.perf_counter()
+    Ks, Ms = nonconi.zpm(kappa, Mb, ps, Qmin, Qmax, 3.0, device=device)
+    wall = time.perf_counter() - t0
+    out = {"workload": f"non-coni Manwe geometry (h11 = 8), {len(ps)} p-vectors (box |p| <= 6), dilation 3, "
+                       f"Qmax {Qmax}",
+           "points": int(len(r[2])), "nodes": int(st["nodes"]), "device_ms": dev_s * 1e3,
+           "stage_ms": {"setup": st["ms_setup"], "search": st["ms_search"], "output": st["ms_output"]},
+           "nodes_per_s": st["nodes"] / dev_s, "directions_per_s": len(ps) / dev_s,
+           "pfvs": int(len(Ks)), "zpm_wall_s": wall, "pfvs_per_s": len(Ks) / wall,
+           "failed": int(np.sum(r[4] != 0))}
+    if ref.available():
+        qmax = onc.qmax_of(Qmax, 3.0)
+
+        def chunk(c):
+            n_pts = n_nodes = 0
+            for p in c:
+                res = onc.ref_points(kappa, Mb, p, Qmax, qmax, return_nodes=True)
+                n_pts += len(res[4])
+                n_nodes += res[5]
+            return n_pts, n_nodes
+        t1 = time.perf_counter()
+        with cf.ThreadPoolExecutor(threads) as ex:
+            parts = list(ex.map(chunk, np.array_split(ps, 8 * threads)))
+        dt = time.perf_counter() - t1
+        out["cpu_reference"] = {"points": int(sum(x[0] for x in parts)), "nodes": int(sum(x[1] for x in parts)),
+                                "seconds": dt, "nodes_per_s": sum(x[1] for x in parts) / dt,
+                                "directions_per_s": len(ps) / dt, "threads": threads,
+                                "what": "oracle/_ref: the reference's pfl_build (coni = 0) + its kernel per "
+                                        "p-vector (ctypes calls, the GIL released)"}
+        out["device_vs_cpu_reference_directions"] = out["directions_per_s"] / out["cpu_reference"]["directions_per_s"]
+    return out
+
+
 def main():
     args = parse()
     world, rank, local, pg = dist_init()
@@ -640,6 +696,7 @@ def main():
         if rank == 0 and world == 1:
             pfv["dataset"] = pfv_rates(gpu, device, threads)
             pfv["coni_zp"] = coni_zp_rates(device, threads)
+            pfv["nonconi_zpm"] = nonconi_rates(device, threads)
     # roofline of the search kernel: executed warp instructions per launch (ncu
     # per-node figure x the launch's nodes) over its CUDA-event time (the
     # search stage: k_flip, a few microseconds, then k_search<double, 1>); the

@@ -161,6 +161,21 @@ int pfg_coni_pfvs(const pfg_input *in, const pfg_options *opt, pfg_pfv_output *o
 /* Free a pfg_pfv_output's arrays (safe on a zeroed struct). */
 void pfg_pfv_output_free(pfg_pfv_output *out);
 
+/* Non-coni ZpM on the device (the reference runs it on the CPU only:
+ * pfvs/nonconi.py:262-514 with its C setup and kernel): for each p-vector
+ * (ps rows hold all h11 entries; p in the Kahler cone), the lattice points c
+ * with c^T mat c <= qmax and the non-strict GCD cut g == 0 or Q g >= q,
+ * g = gcd(K), K = Z M: Z = kappa . p, Binter a basis of {M in the M-lattice :
+ * K . p = 0} LLL-reduced w.r.t. mat = -Binter^T Z Binter (pfl_build with
+ * coni = 0, pfvs/fp_kernel/pfv_lattice.h:554-680, then pfv_kernel,
+ * pfvs/fp_kernel/fp_kernel.pyx:321-352).  in->Q is the search's Qmax and
+ * in->qmax = floor(dilation Qmax); in->linmin is ignored (no M0 cut); the
+ * rows are pfg_coni_batch_ex's (M = Binter c, Kn = Z M, q, pidx, canonical
+ * order) and the options and statistics too.  h11 <= pfg_max_h11() - 1.
+ * Returns 0, or 1 with out->err set. */
+int pfg_zpm_batch(const pfg_input *in, const pfg_options *opt, pfg_output *out, pfg_stats *stats,
+                  int64_t *dir_nodes);
+
 /* The coni dilation bound of n_p directions p_hat = (0, p_r) of one geometry
  * (kappa, h^3): mu0 = min over nonzero K in Z^(h-1) with p_r . K = 0 of
  * -K^T A_rr^-1 K, A = kappa . p_hat, so that every coni PFV with direction

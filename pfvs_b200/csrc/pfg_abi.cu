@@ -337,7 +337,7 @@ extern "C" int pfg_coni_batch(const pfg_input *in, pfg_output *out)
 // The pipeline over all batches: points into `out`, or, with `pfv`, the
 // points' PFVs into `pfv` (the points stay on the device).
 static int coni_run(const pfg_input *in, const pfg_options *opt_in, pfg_output *out, pfg_stats *stats,
-                    int64_t *dir_nodes_out, PfvSink *pfv)
+                    int64_t *dir_nodes_out, PfvSink *pfv, int coni = 1)
 {
     memset(out, 0, sizeof *out);
     if (stats) memset(stats, 0, sizeof *stats);
@@ -364,9 +364,12 @@ static int coni_run(const pfg_input *in, const pfg_options *opt_in, pfg_output *
             Geo &g = geos[gi];
             g.h = in->h[gi];
             g.d = g.h - 1;
-            g.Q = in->Q[gi]; g.qmax = in->qmax[gi]; g.linmin = in->linmin[gi];
-            if (g.h < 3 || g.h > MH || g.Q <= 0 || g.qmax < 0) {
-                set_err(out, "geometry %d: unsupported h11 = %d (3..%d), Q or qmax", gi, g.h, MH);
+            g.Q = in->Q[gi]; g.qmax = in->qmax[gi];
+            g.coni = coni;
+            g.linmin = coni ? in->linmin[gi] : 0;     // (non-coni: no M0 cut)
+            // (a non-coni geometry's GCD rows start from all h rows of ZB: h <= MH - 1)
+            if (g.h < 3 || g.h > MH - (coni ? 0 : 1) || g.Q <= 0 || g.qmax < 0) {
+                set_err(out, "geometry %d: unsupported h11 = %d (3..%d), Q or qmax", gi, g.h, MH - (coni ? 0 : 1));
                 return 1;
             }
             g.use_f32 = g.qmax < (1LL << 22) && opt.precision == PFG_PREC_FP32;
@@ -450,16 +453,19 @@ static int coni_run(const pfg_input *in, const pfg_options *opt_in, pfg_output *
                 todoall[k] = k;
                 if (geos[in->pgeo[off + k]].use_f32) todo32.push_back(k);
             }
-            // setup order: h11 <= 32 (shared-memory LLL) then the rest, each largest h11 first
+            // setup order: the directions whose LLL working set is an LllMem<32> (shared
+            // memory: h11 <= 32, or <= 31 without the coni row) then the rest, each
+            // largest h11 first
             std::vector<int32_t> order(nb);
             for (int k = 0; k < nb; ++k) order[k] = k;
+            auto small = [&](int32_t k) { const Geo &g = geos[in->pgeo[off + k]]; return g.h + (g.coni ? 0 : 1) <= 32; };
             std::stable_sort(order.begin(), order.end(), [&](int32_t a, int32_t b) {
                 const int ha = geos[in->pgeo[off + a]].h, hb = geos[in->pgeo[off + b]].h;
-                if ((ha <= 32) != (hb <= 32)) return ha <= 32;
+                if (small(a) != small(b)) return small(a);
                 return ha > hb;
             });
             int n32 = 0;
-            while (n32 < nb && geos[in->pgeo[off + order[n32]]].h <= 32) ++n32;
+            while (n32 < nb && small(order[n32])) ++n32;
             const int n64 = nb - n32;
             const size_t smem32 = sizeof(LllMem<32>);
             int grid32 = 0, grid64[3] = {0, 0, 0};
@@ -887,6 +893,12 @@ extern "C" int pfg_coni_batch_ex(const pfg_input *in, const pfg_options *opt, pf
                                  pfg_stats *stats, int64_t *dir_nodes)
 {
     return coni_run(in, opt, out, stats, dir_nodes, nullptr);
+}
+
+extern "C" int pfg_zpm_batch(const pfg_input *in, const pfg_options *opt, pfg_output *out, pfg_stats *stats,
+                             int64_t *dir_nodes)
+{
+    return coni_run(in, opt, out, stats, dir_nodes, nullptr, 0);
 }
 
 extern "C" int pfg_coni_pfvs(const pfg_input *in, const pfg_options *opt, pfg_pfv_output *out, pfg_stats *stats)

@@ -146,7 +146,8 @@ template <class R> struct Prob {
     const int64_t *HD;                // staged: the GCD rows' pivots H_ii (0 where no row is kept)
     const int64_t *H;                 // global, transposed: H[c d + r] = entry c of the row with pivot r
     const double *U64, *UI64;         // global: the FP64 factor (d x d row-major), 1/U_ii
-    int d, h, m0_level, pad;
+    int d, h, m0_level;
+    int coni;                         // 1: strict GCD cut on K[1:] (coni); 0: non-strict on all of K
     int64_t g_lin, Q, qmax, linmin;
     uint64_t hrows;
     R qmax_r, slack, Kerr, max_err, invQ;
@@ -181,7 +182,7 @@ template <class R> __device__ Prob<R> load_prob(const SearchArgs &A, int pid, vo
     for (int e = lane; e < d; e += 32) HD[e] = ((D.hrows >> e) & 1) ? s[L.H + (int64_t)e * d + e] : 0;
     __syncwarp();
     Prob<R> P;
-    P.d = d; P.h = h; P.m0_level = D.m0_level;
+    P.d = d; P.h = h; P.m0_level = D.m0_level; P.coni = g.coni;
     P.g_lin = D.g_lin; P.Q = g.Q; P.qmax = g.qmax; P.linmin = g.linmin; P.hrows = D.hrows;
     P.U = U; P.UI = UI; P.MAT = MAT; P.ZT = ZT; P.HD = HD; P.H = s + L.H;
     P.U64 = (const double *)(s + L.u64); P.UI64 = (const double *)(s + L.ui64);
@@ -198,24 +199,25 @@ template <class R> __device__ Prob<R> load_prob(const SearchArgs &A, int pid, vo
     return P;
 }
 
-// smallest gcd that can pass the GCD cut when q >= q_lb (fpk_search_impl.h:43-51);
-// q_lb / Q as a product with the rounded 1/Q: its few units of rounding are far
-// inside the G (1 + t) margin taken off below
-template <class R> __device__ __forceinline__ uint64_t need_of(R q_lb, R invQ)
+// smallest gcd that can pass the GCD cut when q >= q_lb (fpk_search_impl.h:43-51):
+// Q g > q (strict, coni) or Q g >= q (non-coni); q_lb / Q as a product with the
+// rounded 1/Q: its few units of rounding are far inside the G (1 + t) margin
+// taken off below
+template <class R> __device__ __forceinline__ uint64_t need_of(R q_lb, R invQ, int strict)
 {
     if (!(q_lb > 0)) return 0;
     R t = q_lb * invQ;
     t -= Num<R>::G() * ((R)1 + t);
     if (t < 0) t = 0;
     if (t >= (R)1.8e19) return UINT64_MAX;
-    return (uint64_t)floor((double)t) + 1;             // strict cut
+    return strict ? (uint64_t)floor((double)t) + 1 : (uint64_t)ceil((double)t);
 }
-// the branch must fail Q g > q when q >= q_lb (fpk_search_impl.h:56-62)
-template <class R> __device__ __forceinline__ bool gcd_fails(u128 g, int64_t Q, R q_lb)
+// the branch must fail the cut when q >= q_lb (fpk_search_impl.h:56-62)
+template <class R> __device__ __forceinline__ bool gcd_fails(u128 g, int64_t Q, R q_lb, int strict)
 {
     if (g == 0 || (g >> 64) != 0) return false;
     R Qg = (R)Q * (R)(uint64_t)g;
-    return Qg <= q_lb;
+    return strict ? Qg <= q_lb : Qg < q_lb;
 }
 
 struct Tally { unsigned long long nodes, cands, leaves; };
@@ -608,11 +610,11 @@ __device__ int run_subtree(const SearchArgs &A, const Prob<R> &P, int pid, const
         if (pass) {
             const R q_lb = (P.qmax_r - nr) - (slack + en);
             if (hrow) {
-                if (gcd_fails(gn, P.Q, q_lb)) pass = false;
+                if (gcd_fails(gn, P.Q, q_lb, P.coni)) pass = false;
                 else {
                     u128 a = uabs(pre + (i128)hii * v);
                     if ((gn >> 64) == 0 && (a >> 64) == 0 && (gn | a) != 0) {
-                        uint64_t gg = gcd64_ge_small((uint64_t)gn, (uint64_t)a, need_of(q_lb, P.invQ));
+                        uint64_t gg = gcd64_ge_small((uint64_t)gn, (uint64_t)a, need_of(q_lb, P.invQ, P.coni));
                         if (!gg) pass = false;
                         gn = gg;
                     } else {
@@ -620,7 +622,7 @@ __device__ int run_subtree(const SearchArgs &A, const Prob<R> &P, int pid, const
                     }
                 }
             }
-            if (pass && gcd_fails(gn, P.Q, q_lb)) pass = false;
+            if (pass && gcd_fails(gn, P.Q, q_lb, P.coni)) pass = false;
         }
 #ifdef PFG_STAGE_CLOCKS
         __syncwarp();
@@ -673,17 +675,20 @@ __device__ int run_subtree(const SearchArgs &A, const Prob<R> &P, int pid, const
             q = A0 + (i128)2 * v * B0 + (i128)m00 * v * v;
             if (q > (i128)P.qmax) ok = false;
         }
-        unsigned need_g = __ballot_sync(FULL, ok && q >= (i128)P.Q);
-        while (need_g) {                          // Q g > q needs g = gcd(Kn[1:]) exactly
+        // Q g > q (coni: g = gcd(Kn[1:])) or Q g >= q (non-coni: g = gcd(Kn)) needs g exactly
+        // where g = 1 would not already pass
+        unsigned need_g = __ballot_sync(FULL, ok && (P.coni ? q >= (i128)P.Q : q > (i128)P.Q));
+        const int k_lo = P.coni ? 1 : 0;
+        while (need_g) {
             const int t = __ffs(need_g) - 1;
             need_g &= need_g - 1;
             const int64_t vt = cur + t;
             const i128 qt = shfl128(q, t);
             uint64_t g = 0;
-            if (lane >= 1 && lane < h) g = gcd64(g, uabs64(S.k0 + (int64_t)P.ZT[lane] * vt));
+            if (lane >= k_lo && lane < h) g = gcd64(g, uabs64(S.k0 + (int64_t)P.ZT[lane] * vt));
             if (NS > 1 && lane + 32 < h) g = gcd64(g, uabs64(S.k1 + (int64_t)P.ZT[lane + 32] * vt));
             for (int o = 16; o; o >>= 1) g = gcd64(g, __shfl_xor_sync(FULL, g, o));
-            if (g != 0 && (i128)P.Q * (i128)g <= qt && lane == t) ok = false;
+            if (g != 0 && lane == t && (P.coni ? (i128)P.Q * (i128)g <= qt : (i128)P.Q * (i128)g < qt)) ok = false;
         }
         unsigned emit = __ballot_sync(FULL, ok);
 #ifdef PFG_STAGE_CLOCKS

@@ -770,8 +770,12 @@ template <int N> __device__ int setup_phase0(const SetupArgs &A, int pid, int la
     if (warp_any(bad)) return ST_OVERFLOW;
     if (lane == 0) {
         int no = 0;
-        for (int a = 0; a < d; ++a) if (W->S[a * MH] == 0) W->order[no++] = a;
-        for (int a = 0; a < d; ++a) if (W->S[a * MH] != 0) W->order[no++] = a;
+        if (g.coni) {
+            for (int a = 0; a < d; ++a) if (W->S[a * MH] == 0) W->order[no++] = a;
+            for (int a = 0; a < d; ++a) if (W->S[a * MH] != 0) W->order[no++] = a;
+        } else {
+            for (int a = 0; a < d; ++a) W->order[no++] = a;
+        }
     }
     __syncwarp();
     int64_t *BT = slab + L.bt, *ZT = slab + L.zt, *MAT = slab + L.mat;
@@ -817,15 +821,26 @@ template <int N> __device__ int setup_phase1(const SetupArgs &A, int pid, int la
     int64_t *BT = slab + L.bt, *ZT = slab + L.zt, *MAT = slab + L.mat;
     int st = 0;
     clk.mark(8);
-    // 8. cut-aware basis (pfv_lattice.h:554-602)
-    for (int a = lane; a < d; a += 32) W->v[a] = BT[a * h];
-    __syncwarp();
-    bool lnz = false;
-    for (int a = lane; a < d; a += 32) lnz |= W->v[a] != 0;
-    lnz = warp_any(lnz);
+    // 8. cut-aware basis (pfv_lattice.h:554-602); without an M0 cut (a non-coni
+    // geometry) the whole basis LLL-reduced w.r.t. mat instead (pfv_lattice.h:560-566)
+    bool lnz = !g.coni;
+    if (g.coni) {
+        for (int a = lane; a < d; a += 32) W->v[a] = BT[a * h];
+        __syncwarp();
+        for (int a = lane; a < d; a += 32) lnz |= W->v[a] != 0;
+        lnz = warp_any(lnz);
+    }
     int m0_level = -1;
     int64_t g_lin = 0;
-    if (lnz) {
+    if (lnz && !g.coni) {
+        // B = the identity, its Gram w.r.t. mat is mat itself
+        for (int e = lane; e < d * d; e += 32) S->B[(e / d) * N + e % d] = (e / d) == (e % d);
+        for (int e = lane; e < d * d; e += 32) {
+            const int i = e / d, j = e % d;
+            if (j <= i) S->G[gix(i, j)] = (i128)MAT[i * d + j];
+        }
+        __syncwarp();
+    } else if (lnz) {
         if ((st = warp_unimodular(W->v, d, W->V, W->w, W->order, lane))) return st;
         // B rows 0..d-2 = K = V[1..], row d-1 = w = V[0]
         for (int e = lane; e < d * d; e += 32) {
@@ -833,6 +848,8 @@ template <int N> __device__ int setup_phase1(const SetupArgs &A, int pid, int la
             S->B[a * N + c] = a < d - 1 ? W->V[(a + 1) * MH + c] : W->V[c];
         }
         __syncwarp();
+    }
+    if (lnz && g.coni) {
         // Gram w.r.t. mat: G_ij = B_i^T mat B_j  (T holds mat B_j)
         for (int j = 0; j < d; ++j) {
             for (int c = lane; c < d; c += 32) {
@@ -853,9 +870,12 @@ template <int N> __device__ int setup_phase1(const SetupArgs &A, int pid, int la
             __syncwarp();
         }
         if (warp_any(bad)) return ST_OVERFLOW;
+    }
+    if (lnz) {
         {
             Lll<N> LK{S, d, d};
-            if ((st = warp_lll(LK, d - 1, true, PFG_DELTA_K, lane))) {
+            // (coni: the d - 1 rows spanning ker l, then w size-reduced; else all d rows)
+            if ((st = g.coni ? warp_lll(LK, d - 1, true, PFG_DELTA_K, lane) : warp_lll(LK, d, false, PFG_DELTA_K, lane))) {
                 // a non-positive norm under mat: not positive definite when an
                 // integer witness says so (exact), else not decided here
                 if (st == ST_NONPOS)
@@ -888,10 +908,12 @@ template <int N> __device__ int setup_phase1(const SetupArgs &A, int pid, int la
         }
         __syncwarp();
         if (warp_any(bad)) return ST_OVERFLOW;
-        for (int a = lane; a < d - 1; a += 32) bad |= BT[a * h] != 0;
-        if (warp_any(bad)) return ST_OVERFLOW;      // (cannot happen: K spans ker l)
-        m0_level = d - 1;
-        g_lin = BT[(d - 1) * h];
+        if (g.coni) {
+            for (int a = lane; a < d - 1; a += 32) bad |= BT[a * h] != 0;
+            if (warp_any(bad)) return ST_OVERFLOW;      // (cannot happen: K spans ker l)
+            m0_level = d - 1;
+            g_lin = BT[(d - 1) * h];
+        }
     } else if (g.linmin > 0) {
         if (lane == 0) { D.m0_level = -1; D.g_lin = 0; }
         return ST_EMPTY;
@@ -926,12 +948,15 @@ template <int N> __device__ int setup_rows_bounds(const SetupArgs &A, int pid, i
     // are the rows of R with row 0 = p'^T R = 0: drop it, the rest is a basis.
     // (Lanes own columns here, so the row operations need no staging.)  The
     // rows only prune: when one cannot be built, the search goes without it.
+    // (A non-coni geometry cuts on all of K: the rows are those of ZB[0:], their
+    // relation p, and nin = h rows in, h - 1 out; LllMem<N> holds N - 1 >= h rows.)
+    const int r0 = g.coni ? 1 : 0, nin = h - r0;
     if (want_rows) {
         for (int c = lane; c < d; c += 32)
-            for (int r = 0; r < d; ++r) S->B[r * N + c] = ZT[c * h + r + 1];
-        for (int e = lane; e < d; e += 32) W->w[e] = p[e + 1];
+            for (int r = 0; r < nin; ++r) S->B[r * N + c] = ZT[c * h + r + r0];
+        for (int e = lane; e < nin; e += 32) W->w[e] = p[e + r0];
         __syncwarp();
-        for (int k = 1; k < d; ++k) {
+        for (int k = 1; k < nin; ++k) {
             int64_t wk = W->w[k];
             if (wk == 0) continue;
             int64_t w0 = W->w[0], s, t;
@@ -956,7 +981,7 @@ template <int N> __device__ int setup_rows_bounds(const SetupArgs &A, int pid, i
         if (warp_any(bad)) return ST_OVERFLOW;      // p'^T ZB[1:] must vanish exactly
     }
     if (want_rows) {
-        int nr = d - 1;
+        int nr = nin - 1;
         for (int c = lane; c < d; c += 32)          // drop row 0
             for (int r = 0; r < nr; ++r) S->B[r * N + c] = S->B[(r + 1) * N + c];
         __syncwarp();
@@ -1204,7 +1229,7 @@ template <int N, int PH> __global__ void __launch_bounds__(128) k_setup(SetupArg
         }
         __syncwarp();
         int stage = 0;
-        int st = g.h <= N ? setup_phase<N, PH>(A, pid, lane, stage, S) : ST_OVERFLOW;
+        int st = g.h + (g.coni ? 0 : 1) <= N ? setup_phase<N, PH>(A, pid, lane, stage, S) : ST_OVERFLOW;
         if (lane == 0) { A.dirs[pid].status = st; A.dirs[pid].pad = st < 0 ? stage : 0; }
         __syncwarp();
     }

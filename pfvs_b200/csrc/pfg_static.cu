@@ -84,7 +84,7 @@ __global__ void __launch_bounds__(32) k_direction_static(StaticScratch *S, int h
     // everything the previous call left in the scratch that must start from zero
     if (lane == 0) {
         Geo &g = S->geo;
-        g.h = h; g.d = d; g.use_f32 = 0; g.pad = 0;
+        g.h = h; g.d = d; g.use_f32 = 0; g.coni = 1;
         g.Q = Q; g.qmax = qmax; g.linmin = linmin;
         g.koff = 0; g.moff = 0; g.slab_len = L.len;
         S->zero32[0] = 0; S->zero64[0] = 0;

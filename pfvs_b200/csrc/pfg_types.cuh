@@ -30,7 +30,8 @@ enum : int {
 };
 
 struct Geo {
-    int h, d, use_f32, pad;
+    int h, d, use_f32;
+    int coni;                   // 1: coni (M0 cut, strict GCD cut on K[1:]); 0: non-coni (none, non-strict on K)
     int64_t Q, qmax, linmin;
     int64_t koff, moff;         // offsets of kappa (h^3) and Mbasis (h^2)
     int64_t slab_len;           // int64 words of one direction's slab

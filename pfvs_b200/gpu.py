@@ -108,6 +108,8 @@ def _load():
     lib.pfg_coni_batch_ex.argtypes = [ctypes.POINTER(_Input), ctypes.POINTER(_Options),
                                       ctypes.POINTER(_Output), ctypes.POINTER(_Stats), _i64p]
     lib.pfg_coni_batch_ex.restype = ctypes.c_int
+    lib.pfg_zpm_batch.argtypes = lib.pfg_coni_batch_ex.argtypes
+    lib.pfg_zpm_batch.restype = ctypes.c_int
     lib.pfg_output_free.argtypes = [ctypes.POINTER(_Output)]
     lib.pfg_coni_pfvs.argtypes = [ctypes.POINTER(_Input), ctypes.POINTER(_Options),
                                   ctypes.POINTER(_PfvOutput), ctypes.POINTER(_Stats)]
@@ -187,7 +189,7 @@ def _geometry_arrays(geoms, MH):
             raise ValueError(f"the GPU build supports 3 <= h11 <= {MH}")
         Q[k] = int(g["Q"])
         qmax[k] = _qmax(int(Q[k]), g["dilation"])
-        linmin[k] = math.ceil(g["M0min"] - 1e-9)
+        linmin[k] = math.ceil(g.get("M0min", 0) - 1e-9)
         blocks_k.append(kap_k.reshape(-1))
         blocks_m.append(np.ascontiguousarray(g["Mbasis"], dtype=np.int64).reshape(-1))
     kap = np.concatenate(blocks_k) if blocks_k else np.zeros(1, dtype=np.int64)
@@ -278,6 +280,31 @@ def coni_batch_multi_ex(geoms, ps, pgeo, device=0, batch=0, verbose=False,
     bytes copied back) and the call's statistics.  Returns
     (M, Kn, q, pidx, pstat, seconds_gpu, stats dict[, dir_nodes]).
     """
+    return _batch_ex("pfg_coni_batch_ex", geoms, ps, pgeo, device, batch, verbose, form, precision,
+                     blocks_per_sm, warps_per_block, want_dir_nodes, gcd_min_tree, wait_s, deadline_s,
+                     check_fp32, compact_rows)
+
+
+def zpm_batch_multi_ex(geoms, ps, pgeo, device=0, batch=0, verbose=False,
+                       form=FORM_BATCHED, precision=PREC_AUTO, blocks_per_sm=0,
+                       warps_per_block=0, want_dir_nodes=False, gcd_min_tree=0.0,
+                       wait_s=0.0, deadline_s=0.0, check_fp32=False, compact_rows=False):
+    """
+    Non-coni ZpM's lattice points on the device (pfg_zpm_batch): as
+    `coni_batch_multi_ex`, with each geometry's `Q` the search's Qmax
+    (qmax = floor(dilation Qmax); `M0min` is ignored: no M0 cut) and the
+    p-vectors with all h11 entries (any p in the Kahler cone).  The points c
+    satisfy c^T mat c <= qmax and the non-strict GCD cut (g == 0 or
+    Qmax g >= q, g = gcd(K)), as the reference's pfv_kernel
+    (pfvs/fp_kernel/fp_kernel.pyx:321-352) returns them for nonconi.ZpM.
+    """
+    return _batch_ex("pfg_zpm_batch", geoms, ps, pgeo, device, batch, verbose, form, precision,
+                     blocks_per_sm, warps_per_block, want_dir_nodes, gcd_min_tree, wait_s, deadline_s,
+                     check_fp32, compact_rows)
+
+
+def _batch_ex(entry, geoms, ps, pgeo, device, batch, verbose, form, precision, blocks_per_sm,
+              warps_per_block, want_dir_nodes, gcd_min_tree, wait_s, deadline_s, check_fp32, compact_rows):
     lib = _require()
     MH = lib.pfg_max_h11()
     h, Q, qmax, linmin, kap, Mb, P, pgeo, n_p = _pack(geoms, ps, pgeo, MH)
@@ -291,8 +318,8 @@ def coni_batch_multi_ex(geoms, ps, pgeo, device=0, batch=0, verbose=False,
     st = _Stats()
     dn = np.zeros(max(n_p, 1), dtype=np.int64)
     out = _Output()
-    rc = lib.pfg_coni_batch_ex(ctypes.byref(inp), ctypes.byref(opt), ctypes.byref(out),
-                               ctypes.byref(st), dn.ctypes.data_as(_i64p))
+    rc = getattr(lib, entry)(ctypes.byref(inp), ctypes.byref(opt), ctypes.byref(out),
+                             ctypes.byref(st), dn.ctypes.data_as(_i64p))
     if rc != 0:
         raise RuntimeError(f"GPU pipeline failed: {out.err.decode(errors='replace')}")
     width = max(3, int(h.max())) if (compact_rows and len(h)) else MH

@@ -132,36 +132,41 @@ def lll_rows_fast(B, delta=0.99, max_swaps=10**6):
     return B
 
 
-def a_matrix(kappa):
-    """The a-matrix in the coni basis with the coni row dropped
-    (pfvs/cydata.py:252-283): a_ij = kappa_iij (i >= j), kappa_ijj (i < j)."""
+def a_matrix(kappa, coni=True):
+    """The a-matrix (pfvs/cydata.py:252-283): a_ij = kappa_iij (i >= j),
+    kappa_ijj (i < j); in the coni basis with the coni row dropped (coni), or
+    whole (a non-coni geometry)."""
     h = kappa.shape[0]
     a = np.zeros((h, h), dtype=np.int64)
     for x in range(h):
         for y in range(h):
             a[x, y] = kappa[x, x, y] if x >= y else kappa[x, y, y]
-    return a[1:]
+    return a[1:] if coni else a
 
 
-def b_vector(c2):
-    """b = c2 + 2 e0 in the coni basis (pfvs/cydata.py:285-303)."""
+def b_vector(c2, coni=True):
+    """b = c2 + 2 e0 in the coni basis (coni), or c2 (non-coni)
+    (pfvs/cydata.py:285-303)."""
     b = np.array(c2, dtype=np.int64).copy()
-    b[0] += 2
+    if coni:
+        b[0] += 2
     return b
 
 
-def m_lattice(kappa, c2):
+def m_lattice(kappa, c2, coni=True):
     """
     Basis (columns, h x h int64) of {M in Z^h : (a/2) M integral and
     (b/24) . M integral}: the lattice of `CYData.M_lattice`
     (pfvs/cydata.py:307-356), computed by refining Z^h one congruence at
     a time (`refine_congruence`: b . M = 0 mod 24, then each row of a mod 2),
-    LLL-reducing after each step to keep the entries small.
+    LLL-reducing after each step to keep the entries small.  a and b as
+    a_matrix / b_vector for a coni geometry (kappa, c2 in the coni basis) or
+    a non-coni one.
     """
     kappa = np.asarray(kappa, dtype=np.int64)
     h = kappa.shape[0]
-    a = a_matrix(kappa)
-    b = b_vector(c2)
+    a = a_matrix(kappa, coni)
+    b = b_vector(c2, coni)
     B = [[int(i == j) for i in range(h)] for j in range(h)]   # columns of I
     B = refine_congruence(B, [int(x) for x in b], 24)
     for row in a:

@@ -40,13 +40,15 @@ def _load():
         lib.emu_witness_not_pd.restype = ctypes.c_int
         lib.emu_last_fp32_check.argtypes = [ctypes.POINTER(ctypes.c_double)]
         lib.emu_set_gcd_min_tree.argtypes = [ctypes.c_double]
+        lib.emu_set_coni.argtypes = [ctypes.c_int]
         _lib = lib
     return _lib
 
 
-def coni_batch_multi(geoms, ps, pgeo, precision=2, n_warps=2):
+def coni_batch_multi(geoms, ps, pgeo, precision=2, n_warps=2, coni=True):
     """As pfvs_b200.gpu.coni_batch_multi, on the emulated warps (default: FP32
-    pruning with the FP64 retry, so that both search instantiations run).  Returns
+    pruning with the FP64 retry, so that both search instantiations run); with
+    coni False the non-coni ZpM of pfg_zpm_batch (geometry Q = Qmax).  Returns
     (M, Kn, q, pidx, pstat, dir_nodes, setup_failure_stage)."""
     from pfvs_b200 import gpu
     lib = _load()
@@ -60,8 +62,12 @@ def coni_batch_multi(geoms, ps, pgeo, precision=2, n_warps=2):
     out = gpu._Output()
     dn = np.zeros(max(n_p, 1), np.int64)
     dbg = np.zeros(max(n_p, 1), np.int32)
-    rc = lib.emu_coni_batch(ctypes.byref(inp), int(precision), int(n_warps), ctypes.byref(out),
-                            dn.ctypes.data_as(i64p), dbg.ctypes.data_as(i32p))
+    lib.emu_set_coni(int(bool(coni)))
+    try:
+        rc = lib.emu_coni_batch(ctypes.byref(inp), int(precision), int(n_warps), ctypes.byref(out),
+                                dn.ctypes.data_as(i64p), dbg.ctypes.data_as(i32p))
+    finally:
+        lib.emu_set_coni(1)
     if rc:
         raise RuntimeError(out.err.decode())
     try:

@@ -39,6 +39,10 @@ extern "C" void emu_set_gcd_min_tree(double v) { g_emu_gcd_min_tree = v < 0 ? 0.
 static double g_emu_chk[4];
 extern "C" void emu_last_fp32_check(double *out) { memcpy(out, g_emu_chk, sizeof g_emu_chk); }
 
+// 1: the coni pipeline (pfg_coni_batch_ex); 0: non-coni ZpM (pfg_zpm_batch)
+static int g_emu_coni = 1;
+extern "C" void emu_set_coni(int coni) { g_emu_coni = coni; }
+
 // precision: PFG_PREC_*, or 3 for FP32 pruning in the bound-check form
 extern "C" int emu_coni_batch(const pfg_input *in, int precision, int n_warps, pfg_output *out,
                               int64_t *dir_nodes_out, int32_t *dir_debug)
@@ -53,7 +57,9 @@ extern "C" int emu_coni_batch(const pfg_input *in, int precision, int n_warps, p
     for (int gi = 0; gi < in->n_geo; ++gi) {
         Geo &g = geos[gi];
         g.h = in->h[gi]; g.d = g.h - 1;
-        g.Q = in->Q[gi]; g.qmax = in->qmax[gi]; g.linmin = in->linmin[gi];
+        g.Q = in->Q[gi]; g.qmax = in->qmax[gi];
+        g.coni = g_emu_coni;
+        g.linmin = g.coni ? in->linmin[gi] : 0;
         g.use_f32 = g.qmax < (1LL << 22) && precision == PFG_PREC_FP32;
         g.koff = koff; g.moff = moff;
         g.slab_len = slab_layout(g.h, g.d).len;
@@ -78,7 +84,7 @@ extern "C" int emu_coni_batch(const pfg_input *in, int precision, int n_warps, p
     unsigned next = 0;
     // the device's split: h11 <= 32 through the LllMem<32> kernel, the rest through LllMem<64>
     std::vector<int32_t> o32, o64;
-    for (int k = 0; k < nb; ++k) (geos[pgeo[k]].h <= 32 ? o32 : o64).push_back(k);
+    for (int k = 0; k < nb; ++k) (geos[pgeo[k]].h + (g_emu_coni ? 0 : 1) <= 32 ? o32 : o64).push_back(k);
     unsigned next64 = 0;
     SetupArgs SA{geos.data(), in->kappa, in->Mbasis, in->ps, pgeo.data(), slab_off.data(), slab.data(),
                  dirs.data(), scratch.data(), (int)o32.size(), &next, o32.data(), 0, g_emu_gcd_min_tree};
