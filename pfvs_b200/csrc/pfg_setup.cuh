@@ -1038,14 +1038,53 @@ h_done:
     // 11. the search keeps exact sums mat c, ZB c, Binter c in int64 and stages
     // mat and ZB^T as int32: every row of mat and every column of Binter^T and
     // (Z Binter)^T has an absolute sum below 2^31, so with |c| < 2^31 every such
-    // sum (and every partial one) stays below 2^62
+    // sum (and every partial one) stays below 2^62.  A mat beyond that (a long,
+    // thin ellipsoid) is read from the slab instead (Dir.wide), with its sums
+    // bounded through the coordinate ranges below.
+    bool wide = false;
     for (int r = lane; r < d; r += 32) {
         uint64_t s = 0;
         for (int j = 0; j < d; ++j) {
             const uint64_t a = uabs64(MAT[r * d + j]);
-            if (a >= (1ull << 31)) bad = true; else s += a;
+            if (a >= (1ull << 31)) wide = true; else s += a;
         }
-        bad |= s >= (1ull << 31);
+        wide |= s >= (1ull << 31);
+    }
+    wide = warp_any(wide);
+    if (wide) {
+        // Every coordinate value the search visits lies in a level interval of the
+        // ellipsoid |U c|^2 <= rho (rho = qmax plus the pruning slack), so
+        // |c_j| <= sqrt(rho) |row j of U^-1| + 1; the bound is taken twice over
+        // (FP64 rounding of U^-1 is far below that), and then every row's
+        // sum |mat_rj| R_j must stay below 2^62.
+        const double *Uf = (const double *)(slab + L.u64);
+        double *X = W->X;
+        for (int j = 0; j < d; ++j) {
+            for (int i = lane; i <= j; i += 32) {
+                double x;
+                if (i == j) x = 1.0 / Uf[j * d + j];
+                else {
+                    double s = 0.0;
+                    for (int k = i; k < j; ++k) s += X[i * MH + k] * Uf[k * d + j];
+                    x = -s / Uf[j * d + j];
+                }
+                X[i * MH + j] = x;
+            }
+            __syncwarp();
+        }
+        const double rho = 2.0 * ((double)g.qmax + slack_chol) + 16.0;
+        for (int j = lane; j < d; j += 32) {
+            double rn = 0.0;
+            for (int k = j; k < d; ++k) rn += X[j * MH + k] * X[j * MH + k];
+            const double rj = 2.0 * sqrt(rho * rn) + 2.0;
+            W->w[j] = rj < 2147483648.0 && rj == rj ? (int64_t)ceil(rj) : (int64_t)(1ll << 31);
+        }
+        __syncwarp();
+        for (int r = lane; r < d; r += 32) {
+            u128 s = 0;
+            for (int j = 0; j < d; ++j) s += (u128)uabs64(MAT[r * d + j]) * (uint64_t)W->w[j];
+            bad |= s >= ((u128)1 << 62);
+        }
     }
     for (int r = lane; r < h; r += 32) {
         uint64_t sb = 0, sz = 0;
@@ -1060,6 +1099,7 @@ h_done:
     if (lane == 0) {
         D.hrows = hrows;
         D.slack_chol = slack_chol;
+        D.wide = wide;
     }
     __syncwarp();
     return ST_PENDING;
@@ -1222,7 +1262,7 @@ template <int N, int PH> __global__ void __launch_bounds__(128) k_setup(SetupArg
             if (lane == 0) {
                 Dir &D = A.dirs[pid];
                 D.geo = A.pgeo[pid]; D.h = g.h; D.d = g.h - 1; D.slab = A.slab_off[pid];
-                D.m0_level = -1; D.g_lin = 0; D.hrows = 0; D.slack_chol = 0.0;
+                D.m0_level = -1; D.g_lin = 0; D.hrows = 0; D.slack_chol = 0.0; D.wide = 0;
             }
         } else if (A.dirs[pid].status != (PH == 3 ? ST_WANT_ROWS : ST_PENDING)) {
             continue;

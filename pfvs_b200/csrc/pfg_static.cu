@@ -92,7 +92,7 @@ __global__ void __launch_bounds__(32) k_direction_static(StaticScratch *S, int h
         S->dir_nodes[0] = 0;
         Dir &D = S->dir;
         D.geo = 0; D.h = h; D.d = d; D.slab = 0; D.status = ST_PENDING;
-        D.m0_level = -1; D.g_lin = 0; D.hrows = 0; D.slack_chol = 0.0; D.pad = 0;
+        D.m0_level = -1; D.g_lin = 0; D.hrows = 0; D.slack_chol = 0.0; D.pad = 0; D.wide = 0;
     }
     __syncwarp();
     // setup (the batch kernel's per-direction step, pfg_setup.cuh)

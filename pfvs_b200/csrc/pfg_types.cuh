@@ -42,6 +42,8 @@ struct Dir {
     int geo, h, d, status;
     int m0_level;               // level at which M0 is determined (-1: M0 == 0)
     int pad;                    // setup step that failed (diagnostics), else 0
+    int wide;                   // 1: mat has entries beyond int32 (the search reads it from the slab)
+    int pad2;
     int64_t g_lin;              // M0 = g_lin * c[d-1] (cut-aware basis)
     uint64_t hrows;             // bit j: the GCD row with pivot j is kept
     int64_t slab;               // offset (int64 words) of the slab

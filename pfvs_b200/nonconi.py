@@ -43,6 +43,18 @@ class IncompleteSearchError(RuntimeError):
     pfvs.util.IncompleteSearchError)."""
 
 
+def _pow_mod(x, e, p):
+    """x^e mod p elementwise (int64, p < 2^31: every product below 2^62)."""
+    r = np.ones_like(x)
+    b = x % p
+    while e:
+        if e & 1:
+            r = (r * b) % p
+        b = (b * b) % p
+        e >>= 1
+    return r
+
+
 def _det_mod(Ns, p):
     """det(N) mod p for a stack of integer matrices (n, m, m), entries < 2^62."""
     A = np.mod(np.asarray(Ns, dtype=np.int64), p)
@@ -62,7 +74,7 @@ def _det_mod(Ns, p):
         det = np.where(swap, (p - det) % p, det)
         pv = A[:, k, k]
         det = (det * pv) % p
-        inv = np.array([pow(int(x), p - 2, p) if x else 0 for x in pv], dtype=np.int64)
+        inv = _pow_mod(pv, p - 2, p)                 # (Fermat; 0 stays 0)
         for i in range(k + 1, m):
             f = (A[:, i, k] * inv) % p
             # row_i -= f row_k (mod p), products below 2^62
@@ -97,7 +109,10 @@ def singular_mask(Ns):
         return np.array([_det_exact(N) == 0 for N in Ns], dtype=bool)
     nonzero = np.zeros(Ns.shape[0], dtype=bool)
     for p in PRIMES:
-        nonzero |= _det_mod(Ns, p) != 0
+        todo = np.flatnonzero(~nonzero)
+        if not len(todo):
+            break
+        nonzero[todo] = _det_mod(Ns[todo], p) != 0
     sing = ~nonzero
     for i in np.flatnonzero(sing):
         sing[i] = _det_exact(Ns[i]) == 0
@@ -123,16 +138,21 @@ def _adjugate(Mb):
 
 def _primitive(M, Mbasis):
     """gcd(c) == 1 for each row M = Mbasis x (x = the coordinates in the
-    M-lattice basis, with gcd(x) = gcd(c))."""
+    M-lattice basis, with gcd(x) = gcd(c)): gcd(adj(Mbasis) M) == |det|."""
     adj, det = _adjugate(np.asarray(Mbasis))
-    A = np.array(adj, dtype=object)
-    X = (A @ M.astype(object).T).T                      # det x
+    h = len(adj)
+    amax = max(abs(v) for r in adj for v in r)
+    if len(M) and amax * int(np.max(np.abs(M))) * h < 2 ** 62:
+        X = np.asarray(M, dtype=np.int64) @ np.array(adj, dtype=np.int64).T      # det x, exact in int64
+        return np.gcd.reduce(np.abs(X), axis=1) == abs(det)
+    X = (np.array(adj, dtype=object) @ np.asarray(M).astype(object).T).T
     g = np.array([math.gcd(*[int(v) for v in row]) for row in X], dtype=object)
     return np.array([int(x) == abs(det) for x in g], dtype=bool)
 
 
 def pfvs_from_points(M, Kn, kappa, Mbasis, Qmin, Qmax):
-    """(Ks, Ms) of lattice points (M, Kn = Z M rows), as nonconi.py:432-497."""
+    """(Ks, Ms) of lattice points (M, Kn = Z M rows), as nonconi.py:432-497,
+    of any number of p-vectors at once (each point's test is its own)."""
     h = np.asarray(kappa).shape[0]
     M, Kn = np.asarray(M)[:, :h], np.asarray(Kn)[:, :h]
     empty = (np.zeros((0, h), np.int64), np.zeros((0, h), np.int64))
@@ -149,29 +169,43 @@ def pfvs_from_points(M, Kn, kappa, Mbasis, Qmin, Qmax):
         Ns = np.einsum("abc,nc->nab", kap.astype(object), M.astype(object))
     sing = singular_mask(Ns)
     M, Kn = M[~sing], Kn[~sing]
+    if not len(M):
+        return empty
     g = np.gcd.reduce(np.abs(Kn), axis=1)
     K = Kn // g[:, None]
-    Q = -np.sum(K.astype(object) * M.astype(object), axis=1)
-    inq = np.array([Qmin <= int(q) <= Qmax for q in Q], dtype=bool)
+    if np.max(np.abs(K)) * np.max(np.abs(M)) * h < 2 ** 62:
+        Q = -np.einsum("ij,ij->i", K, M)
+    else:
+        Q = -np.sum(K.astype(object) * M.astype(object), axis=1)
+    inq = np.array([Qmin <= int(q) <= Qmax for q in Q], dtype=bool) if Q.dtype == object else \
+        (Q >= Qmin) & (Q <= Qmax)
     return K[inq].astype(np.int64), M[inq].astype(np.int64)
 
 
 def allow_gcds(Ks, Ms, Qmax, h11):
     """Every (a K, b M), a, b >= 1, with -a b K.M <= Qmax (nonconi.py:50-84),
-    sorted by (K, M).  A pair with -K.M <= 0 has no multiples (the reference's
-    numpy Qmax // 0 is 0)."""
-    out = set()
-    for K, M in zip(Ks, Ms):
-        q = -int(np.dot(np.asarray(K, dtype=object), np.asarray(M, dtype=object)))
-        if q <= 0:
-            continue
-        for a in range(1, Qmax // q + 1):
-            for b in range(1, Qmax // (a * q) + 1):
-                out.add(tuple(int(a * x) for x in K) + tuple(int(b * x) for x in M))
-    if not out:
+    each once, sorted by (K, M).  A pair with -K.M <= 0 has no multiples (the
+    reference's numpy Qmax // 0 is 0)."""
+    Ks, Ms = np.asarray(Ks, dtype=np.int64).reshape(-1, h11), np.asarray(Ms, dtype=np.int64).reshape(-1, h11)
+    q = -np.einsum("ij,ij->i", Ks.astype(object), Ms.astype(object)) if len(Ks) else np.zeros(0, object)
+    ok = np.array([int(x) > 0 for x in q], dtype=bool)
+    Ks, Ms = Ks[ok], Ms[ok]
+    q = np.array([int(x) for x in q[ok]], dtype=np.int64)
+    parts = []
+    for a in range(1, int(Qmax) + 1):
+        sel = a * q <= Qmax
+        if not sel.any():
+            break
+        Ka, Ma, qa = Ks[sel] * a, Ms[sel], q[sel] * a
+        for b in range(1, int(Qmax) // a + 1):
+            sb = b * qa <= Qmax
+            if not sb.any():
+                break
+            parts.append(np.hstack([Ka[sb], Ma[sb] * b]))
+    if not parts:
         z = np.zeros((0, h11), dtype=np.int64)
         return z, z.copy()
-    A = np.array(sorted(out), dtype=np.int64)
+    A = np.unique(np.vstack(parts), axis=0)
     return A[:, :h11], A[:, h11:]
 
 
@@ -194,14 +228,8 @@ def zpm(kappa, Mbasis, ps, Qmin, Qmax, dilation, device=0, max_N_pfvs=1_000_000_
         st = int(pstat[i]) if pstat[i] else -2
         raise IncompleteSearchError(f"p={ps[i].tolist()}: the device search returned status {st} "
                                     f"({STATUS_TEXT.get(st, 'not finished')})")
-    Ks, Ms = [], []
-    starts = np.searchsorted(pidx, np.arange(len(ps) + 1))      # (points grouped by p-vector)
-    for i in range(len(ps)):
-        lo, hi = starts[i], starts[i + 1]
-        K, Mm = pfvs_from_points(M[lo:hi], Kn[lo:hi], kappa, Mbasis, Qmin, Qmax)
-        Ks.append(K)
-        Ms.append(Mm)
-    Ks, Ms = allow_gcds(np.vstack(Ks), np.vstack(Ms), int(Qmax), h)
+    K, Mm = pfvs_from_points(M, Kn, kappa, Mbasis, Qmin, Qmax)     # (every point's test is its own)
+    Ks, Ms = allow_gcds(K, Mm, int(Qmax), h)
     if return_info:
         return Ks, Ms, dict(stats, points=int(len(q)), seconds_gpu=secs)
     return Ks, Ms

@@ -8,9 +8,8 @@ non-coni Manwe test geometry, points from its own C setup and kernel):
   the canonical order, with FP64 and with FP32 pruning, all cases in one
   multi-geometry call;
 - the PFVs through the product's post-processing equal the reference
-  route's set, and contain each paper vacuum the device can take (6.4's
-  mat is beyond the search's int32 staging: status -20, raised as an
-  IncompleteSearchError);
+  route's set, and contain each paper vacuum (6.4's mat, beyond the
+  search's int32 staging, is read from the slab);
 - a larger batch (the Manwe geometry's 11,386 primitive p-vectors of the
   box |p| <= 6, at dilation 3) equals the reference's C code on a sample
   and its points are independent of the search form.
@@ -29,7 +28,6 @@ pytestmark = pytest.mark.gpu
 
 G = np.load(os.path.join(ROOT, "tests", "golden", "nonconi.npz"))
 CASES = list(range(int(G["n_cases"][0])))
-WIDE = {3}
 
 
 def _need_gpu():
@@ -64,9 +62,6 @@ def test_device_points_equal_reference_all_cases_in_one_call(precision):
         h = kappa.shape[0]
         n = len(G[f"c{k}_ps"])
         mine = (pidx >= base[k]) & (pidx < base[k] + n)
-        if k in WIDE:
-            assert np.all(pstat[base[k]:base[k] + n] == -20) and not mine.any()
-            continue
         assert np.all(pstat[base[k]:base[k] + n] == 0)
         got = _rows(M[mine], Kn[mine], q[mine], pidx[mine] - base[k], h)
         want = _rows(G[f"c{k}_M"], G[f"c{k}_Kn"], G[f"c{k}_q"], G[f"c{k}_pidx"], h)
@@ -77,10 +72,6 @@ def test_device_points_equal_reference_all_cases_in_one_call(precision):
 def test_device_pfvs_equal_reference(k):
     _need_gpu()
     kappa, Mb, ps, Qmin, Qmax, D = _case(k)
-    if k in WIDE:
-        with pytest.raises(nonconi.IncompleteSearchError, match="status -20"):
-            nonconi.zpm(kappa, Mb, ps, Qmin, Qmax, D)
-        return
     Ks, Ms = nonconi.zpm(kappa, Mb, ps, Qmin, Qmax, D)
     got = {(tuple(int(x) for x in a), tuple(int(x) for x in b)) for a, b in zip(Ks, Ms)}
     want = {(tuple(int(x) for x in a), tuple(int(x) for x in b)) for a, b in zip(G[f"c{k}_pfvK"], G[f"c{k}_pfvM"])}
