@@ -16,6 +16,16 @@ typedef unsigned __int128 u128;
 #else
 #define PFG_NOINLINE __noinline__
 #endif
+// The LLL's inner steps (Gram-Schmidt row, size reduction, swap), inlined into
+// the one out-of-line LLL: called once per loop iteration, a call there costs
+// the saving and restoring of live registers through local memory.
+#ifndef PFG_LLL_INLINE
+#ifdef PFG_EMU
+#define PFG_LLL_INLINE
+#else
+#define PFG_LLL_INLINE __forceinline__
+#endif
+#endif
 
 // PFG_UNIFORM(v): v must be equal in all lanes of the warp (a warp-uniform
 // branch input).  Checked only under the test-suite's CPU warp emulator.

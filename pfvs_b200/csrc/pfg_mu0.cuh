@@ -147,6 +147,7 @@ struct Mu0Scratch {
     int64_t Gr[32 * 32];                      // the reduced integral form
     double R[32 * 32];                        // its FP64 Cholesky factor
     LllMem<32> L;                             // LLL working set (basis of Lambda in O's coordinates)
+    int64_t Lb[31 * 32];                      // its rows
 };
 
 struct Mu0Args {
@@ -466,6 +467,8 @@ __global__ void __launch_bounds__(128) k_mu0(Mu0Args P)
 {
     const int lane = threadIdx.x & 31;
     Mu0Scratch *W = P.scratch + (blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5));
+    if (lane == 0) W->L.B = W->Lb;
+    __syncwarp();
     for (;;) {
         unsigned t = 0;
         if (lane == 0) t = atomicAdd(P.next, 1u);

@@ -143,13 +143,13 @@ template <class R> PFG_HD unsigned stage_bytes(int d, int h)
 template <class R> struct Prob {
     const R *U, *UI;                  // staged: U packed (upk), 1/U_ii
     const int32_t *MAT, *ZT;          // staged: mat (d x d), ZT (d x h)
-    const int64_t *MATg;              // global: mat in int64 (read instead of MAT when wide)
     const int64_t *HD;                // staged: the GCD rows' pivots H_ii (0 where no row is kept)
     const int64_t *H;                 // global, transposed: H[c d + r] = entry c of the row with pivot r
     const double *U64, *UI64;         // global: the FP64 factor (d x d row-major), 1/U_ii
     int d, h, m0_level;
     int coni;                         // 1: strict GCD cut on K[1:] (coni); 0: non-strict on all of K
-    int wide;                         // mat has entries beyond int32: MATg, not MAT
+    int wide;                         // mat has entries beyond int32: read in int64 from the slab,
+                                      // where it lies just before H (H - d d), not from MAT
     int64_t g_lin, Q, qmax, linmin;
     uint64_t hrows;
     R qmax_r, slack, Kerr, max_err, invQ;
@@ -184,7 +184,7 @@ template <class R> __device__ Prob<R> load_prob(const SearchArgs &A, int pid, vo
     for (int e = lane; e < d; e += 32) HD[e] = ((D.hrows >> e) & 1) ? s[L.H + (int64_t)e * d + e] : 0;
     __syncwarp();
     Prob<R> P;
-    P.d = d; P.h = h; P.m0_level = D.m0_level; P.coni = g.coni; P.wide = D.wide; P.MATg = MATg;
+    P.d = d; P.h = h; P.m0_level = D.m0_level; P.coni = g.coni; P.wide = D.wide;
     P.g_lin = D.g_lin; P.Q = g.Q; P.qmax = g.qmax; P.linmin = g.linmin; P.hrows = D.hrows;
     P.U = U; P.UI = UI; P.MAT = MAT; P.ZT = ZT; P.HD = HD; P.H = s + L.H;
     P.U64 = (const double *)(s + L.u64); P.UI64 = (const double *)(s + L.ui64);
@@ -262,8 +262,8 @@ template <class R, int NS> __device__ __forceinline__ void apply_dc(Lanes<R> &S,
 {
     if (dv == 0 || i == 0) return;
     const int d = P.d, h = P.h;
-    if (lane < d) S.y0 += (P.wide ? P.MATg[i * d + lane] : (int64_t)P.MAT[i * d + lane]) * dv;
-    if (NS > 1 && lane + 32 < d) S.y1 += (P.wide ? P.MATg[i * d + lane + 32] : (int64_t)P.MAT[i * d + lane + 32]) * dv;
+    if (lane < d) S.y0 += (P.wide ? P.H[(i - d) * d + lane] : (int64_t)P.MAT[i * d + lane]) * dv;
+    if (NS > 1 && lane + 32 < d) S.y1 += (P.wide ? P.H[(i - d) * d + lane + 32] : (int64_t)P.MAT[i * d + lane + 32]) * dv;
     if (lane < h) S.k0 += (int64_t)P.ZT[i * h + lane] * dv;
     if (NS > 1 && lane + 32 < h) S.k1 += (int64_t)P.ZT[i * h + lane + 32] * dv;
     if (lane < i && ((P.hrows >> lane) & 1)) S.hp0 += (i128)P.H[i * d + lane] * dv;
@@ -499,7 +499,7 @@ __device__ int run_subtree(const SearchArgs &A, const Prob<R> &P, int pid, const
     i128 A0 = 0;
     int64_t B0 = 0;
     if (i == 0) leaf_data<R, NS>(S, P, lane, A0, B0);
-    const int64_t m00 = P.wide ? P.MATg[0] : (int64_t)P.MAT[0];
+    const int64_t m00 = P.wide ? P.H[-(int64_t)P.d * P.d] : (int64_t)P.MAT[0];
     unsigned poll = 0;
     const unsigned long long t0 = shfl(gtimer(), 0);
 #ifdef PFG_STAGE_CLOCKS

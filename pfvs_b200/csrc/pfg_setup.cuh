@@ -38,7 +38,10 @@ template <int N> struct LllMem {
     static constexpr int R = N - 1;             // rows: at most d = h11 - 1 <= N - 1 are ever used
                                                 // (d basis rows in step 4; d - 1 plus the 'last'
                                                 // row in step 8; fewer in step 9)
-    int64_t B[R * N];                           // rows, stride N
+    int64_t *B;                                 // rows, stride N: R * N words in the warp's global
+                                                // scratch (set by the owner), so that the shared-memory
+                                                // working set of h11 <= 32 is only the Gram and
+                                                // Gram-Schmidt data (12.9 KB: 16 warps per SM)
     i128 G[R * (R + 1) / 2];                    // exact Gram, lower triangle packed (gix)
     i128 T[R];                                  // a copied column of G / a temporary vector
     double mu[R * (R - 1) / 2];                 // Gram-Schmidt coefficients mu(k, j), j < k (mix)
@@ -68,6 +71,7 @@ struct SetupScratch {
     int64_t w[MH], v[MH];
     int order[MH];
     LllMem<MH> core;
+    int64_t Bstore[(MH - 1) * MH];  // the rows of the warp's LllMem (core or the shared-memory one)
 };
 
 struct SetupArgs {
@@ -181,7 +185,7 @@ template <int N> struct Lll {
 // r_l (forward substitution by columns, lanes own rows); afterwards lane l
 // holds r_l, so mu_kl = r_l / bb_l and bb_k = G_kk - sum_l mu_kl r_l are
 // formed in parallel.
-template <int N> PFG_NOINLINE __device__ void lll_gs(LllMem<N> *S, int k, int lane)
+template <int N> PFG_LLL_INLINE __device__ void lll_gs(LllMem<N> *S, int k, int lane)
 {
     PFG_T0(t_gs);
     PFG_COUNT(12, 1);
@@ -219,7 +223,7 @@ template <int N> PFG_NOINLINE __device__ void lll_gs(LllMem<N> *S, int k, int la
 // Gram-Schmidt row (Babai), then b_k -= sum_j q_j b_j in one exact pass over
 // B and G; repeated until no multiplier is non-zero.  Leaves row k's
 // Gram-Schmidt data current.
-template <int N> PFG_NOINLINE __device__ int lll_reduce(Lll<N> &L, int k, int lane)
+template <int N> PFG_LLL_INLINE __device__ int lll_reduce(Lll<N> &L, int k, int lane)
 {
     LllMem<N> *S = L.S;
     for (int pass = 0; pass < 16; ++pass) {
@@ -328,7 +332,7 @@ template <int N> PFG_NOINLINE __device__ int lll_reduce(Lll<N> &L, int k, int la
 
 // Exchange rows k-1 and k: B, G exactly; the Gram-Schmidt data of the two
 // rows by the usual update formulas (rows > k are recomputed when visited).
-template <int N> PFG_NOINLINE __device__ void lll_swap(Lll<N> &L, int k, int lane)
+template <int N> PFG_LLL_INLINE __device__ void lll_swap(Lll<N> &L, int k, int lane)
 {
     LllMem<N> *S = L.S;
     for (int c = lane; c < L.n; c += 32) {
@@ -1250,6 +1254,8 @@ template <int N, int PH> __global__ void __launch_bounds__(128) k_setup(SetupArg
     const int lane = threadIdx.x & 31;
     SetupScratch *Wg = A.scratch + (blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5));
     LllMem<N> *S = A.smem_core ? (LllMem<N> *)smem_raw + (threadIdx.x >> 5) : (LllMem<N> *)&Wg->core;
+    if (lane == 0) S->B = Wg->Bstore;
+    __syncwarp();
     const unsigned n = A.n_dev ? *A.n_dev : (unsigned)A.n;
     for (;;) {
         unsigned t = 0;

@@ -98,6 +98,8 @@ __global__ void __launch_bounds__(32) k_direction_static(StaticScratch *S, int h
     // setup (the batch kernel's per-direction step, pfg_setup.cuh)
     SetupArgs SA{&S->geo, kappa, Mbasis, p, S->zero32, S->zero64, S->slab, &S->dir, &S->setup, 1, nullptr};
     int stage = 0;
+    if (lane == 0) S->setup.core.B = S->setup.Bstore;
+    __syncwarp();
     int st = setup_one<MH>(SA, 0, lane, stage, &S->setup.core);
     if (lane == 0) { S->dir.status = st; S->dir.pad = st < 0 ? stage : 0; }
     __syncwarp();

@@ -70,7 +70,7 @@ PFG_HD Slab slab_layout(int h, int d)
     s.bt = 0;
     s.zt = s.bt + (int64_t)d * h;
     s.mat = s.zt + (int64_t)d * h;
-    s.H = s.mat + (int64_t)d * d;
+    s.H = s.mat + (int64_t)d * d;               // (the search reads a wide mat as H - d d)
     s.u64 = s.H + (int64_t)d * d;
     s.u32 = s.u64 + (int64_t)d * d;
     s.ui64 = s.u32 + ((int64_t)d * d + 1) / 2;
