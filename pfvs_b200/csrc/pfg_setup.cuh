@@ -1244,7 +1244,9 @@ template <int N> __device__ int setup_one(const SetupArgs &A, int pid, int lane,
 // phase finished.  N = 32 serves h11 <= 32 with the LLL working set in
 // dynamic shared memory (one LllMem<32> per warp) when A.smem_core is set;
 // otherwise (and for N = 64) the working set is the warp's global scratch.
-template <int N, int PH> __global__ void __launch_bounds__(128) k_setup(SetupArgs A)
+// (N = 32: launched as one-warp blocks, 16 per SM -- 128 registers a thread,
+// 16 x 12.9 KB of shared memory; N = 64: blocks of 4 warps, 4 per SM)
+template <int N, int PH> __global__ void __launch_bounds__(N == 32 ? 32 : 128, N == 32 ? 16 : 4) k_setup(SetupArgs A)
 {
 #ifdef PFG_EMU
     unsigned char *smem_raw = nullptr;
