@@ -56,12 +56,13 @@ sys.path.insert(0, ROOT)
 # figures from one ncu --set full capture of the timed form's search on the
 # first 16,384 directions of this batch (20,582,107 nodes): executed warp
 # instructions and DRAM bytes per search node.
-SEARCH_INST_PER_NODE = 14_977_918_824 / 20_582_107
-SEARCH_DRAM_PER_NODE = (248_137_216 + 110_171_648) / 20_582_107
-# The setup's three phase kernels (k_setup<32, 0..2>) together, from the
-# same kind of capture on the same 16,384 directions: per direction.
-SETUP_INST_PER_DIR = (3_785_943_035 + 6_529_456_061 + 1_841_800_499) / 16384
-SETUP_DRAM_PER_DIR = (10_734_080 + 253_480_192 + 191_088_384 + 196_837_376 + 215_589_376 + 138_622_720) / 16384
+SEARCH_INST_PER_NODE = 14_623_364_332 / 20_582_107
+SEARCH_DRAM_PER_NODE = (247_203_072 + 110_007_296) / 20_582_107
+# The setup's four phase kernels (k_setup<32, 0..3>) together, from the
+# same capture on the same 16,384 directions: per direction.
+SETUP_INST_PER_DIR = (3_753_500_525 + 6_287_646_566 + 255_177_793 + 1_542_075_343) / 16384
+SETUP_DRAM_PER_DIR = (112_741_632 + 255_599_360 + 223_871_488 + 14_464_000
+                      + 389_978_624 + 317_645_312 + 138_759_936 + 402_688) / 16384
 N_SM, SCHEDULERS = 148, 4
 
 
@@ -716,11 +717,11 @@ def main():
     setup_s = per_step["ms_setup"] / 1e3
     n_here = len(idx) / world
     setup_ach = SETUP_INST_PER_DIR * n_here / setup_s
-    roofline_setup = {"kernel": "k_setup<32, 0..2>", "bound": "issue", "achieved": setup_ach, "peak": peak,
+    roofline_setup = {"kernel": "k_setup<32, 0..3>", "bound": "issue", "achieved": setup_ach, "peak": peak,
                       "unit": "warp-inst/s", "frac": setup_ach / peak,
                       "traffic": SETUP_DRAM_PER_DIR * n_here,
                       "basis": f"ncu: {SETUP_INST_PER_DIR:.0f} warp-inst and {SETUP_DRAM_PER_DIR:.0f} DRAM bytes "
-                               f"per direction over the three phases x {n_here:.0f} directions"}
+                               f"per direction over the four phases x {n_here:.0f} directions"}
     failed_all = {str(k): int(allsum(pg, v)) for k, v in sorted(failed.items())}
     failed_step = {str(k): allsum(pg, v) / args.steps for k, v in sorted(failed_timed.items())}
     if rank == 0:
