@@ -17,7 +17,7 @@ use_c_kernel), restated:
                                (c, M = Binter c, Kn = ZB c, q)
   pfvs_from_points(C, M, Kn, kappa, Qmin, Qmax)
                                the reference's per-p post-processing
-                               (nonconi.py:432-497): primitive c only,
+                               (nonconi.py:437-495): primitive c only,
                                det(kappa.M) != 0, K = Z M / gcd, Qmin <= -K.M <= Qmax
   allow_gcds(Ks, Ms, Qmax, h11) nonconi.py:50-84
   zpm(kappa, Mbasis, ps, Qmin, Qmax, dilation) -> set of (K, M) tuples
@@ -126,7 +126,7 @@ def ref_points(kappa, Mbasis, p, Qmax, qmax, eps=1e-4, max_out=10 ** 9, return_n
 
 
 def pfvs_from_points(C, M, Kn, kappa, Qmin, Qmax):
-    """(Ks, Ms) of one p-vector's points, as nonconi.py:432-497 (rows)."""
+    """(Ks, Ms) of one p-vector's points, as nonconi.py:437-495 (rows)."""
     h = np.asarray(kappa).shape[0]
     if not len(C):
         return np.zeros((0, h), np.int64), np.zeros((0, h), np.int64)

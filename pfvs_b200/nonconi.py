@@ -6,7 +6,7 @@ whole basis LLL-reduced w.r.t. mat, the non-strict GCD cut on all of K),
 for every p-vector of a batch at once; the reference runs them on the CPU,
 one p-vector at a time.
 
-The post-processing is the reference's per-p host step (nonconi.py:432-497),
+The post-processing is the reference's per-p host step (nonconi.py:437-495),
 in exact integer numpy: primitive lattice points only (gcd(c) = 1, read off
 M in the M-lattice basis: c and M's coordinates there have the same gcd,
 since Binter spans a saturated sublattice), det(kappa . M) != 0 decided
@@ -151,7 +151,7 @@ def _primitive(M, Mbasis):
 
 
 def pfvs_from_points(M, Kn, kappa, Mbasis, Qmin, Qmax):
-    """(Ks, Ms) of lattice points (M, Kn = Z M rows), as nonconi.py:432-497,
+    """(Ks, Ms) of lattice points (M, Kn = Z M rows), as nonconi.py:437-495,
     of any number of p-vectors at once (each point's test is its own)."""
     h = np.asarray(kappa).shape[0]
     M, Kn = np.asarray(M)[:, :h], np.asarray(Kn)[:, :h]
