@@ -103,6 +103,22 @@ def coni_batch_devices(geoms, ps, pgeo, devices, chunk=8192):
     same order; seconds_gpu is the largest per-device total.
     """
     from . import gpu
+    return _batch_devices(lambda g, p, pg, dev: gpu.coni_batch_multi(g, p, pg, device=dev),
+                          geoms, ps, pgeo, devices, chunk)
+
+
+def zpm_batch_devices(geoms, ps, pgeo, devices, chunk=8192, **opts):
+    """
+    Non-coni ZpM's points (`gpu.zpm_batch_multi_ex`) over several GPUs of
+    this process, as `coni_batch_devices`: (M, Kn, q, pidx, pstat,
+    seconds_gpu) in the one-call order.
+    """
+    from . import gpu
+    return _batch_devices(lambda g, p, pg, dev: gpu.zpm_batch_multi_ex(g, p, pg, device=dev, **opts)[:6],
+                          geoms, ps, pgeo, devices, chunk)
+
+
+def _batch_devices(call, geoms, ps, pgeo, devices, chunk):
     pgeo = np.ascontiguousarray(pgeo, dtype=np.int32)
     bounds = chunk_bounds(len(pgeo), chunk)
     queue = LocalQueue()
@@ -113,7 +129,7 @@ def coni_batch_devices(geoms, ps, pgeo, devices, chunk=8192):
         def one(k):
             lo, hi = bounds[k]
             sub_ps, sub_pgeo = _subset(ps, pgeo, lo, hi)
-            M, Kn, q, pidx, pstat, s = gpu.coni_batch_multi(geoms, sub_ps, sub_pgeo, device=dev)
+            M, Kn, q, pidx, pstat, s = call(geoms, sub_ps, sub_pgeo, dev)
             return (M, Kn, q, pidx, pstat), s
         try:
             got = run_chunks(queue, len(bounds), one)
@@ -134,5 +150,5 @@ def coni_batch_devices(geoms, ps, pgeo, devices, chunk=8192):
     if errors:
         raise errors[0]
     if not bounds:
-        return gpu.coni_batch_multi(geoms, ps, pgeo, device=int(devices[0]))
+        return call(geoms, ps, pgeo, int(devices[0]))
     return gather_points(parts, bounds) + (max(secs.values()) if secs else 0.0,)

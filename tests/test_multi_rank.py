@@ -120,3 +120,34 @@ def test_local_queue_hands_each_chunk_out_once():
     assert sorted(seen) == list(range(500))
     bounds = multi.chunk_bounds(1001, 100)
     assert bounds[0] == (0, 100) and bounds[-1] == (1000, 1001) and len(bounds) == 11
+
+
+def test_nonconi_devices_gather_equals_one_call(monkeypatch):
+    """zpm_batch_devices over three (host-thread) devices, each chunk's points
+    from the reference's non-coni C setup and kernel standing in for the
+    device call: the gathered points equal one call's, in p order."""
+    from oracle import nonconi, ref
+    from pfvs_b200 import gpu, multi
+    if not ref.available():
+        pytest.skip("oracle/_ref not built")
+    G = np.load(os.path.join(ROOT, "tests", "golden", "nonconi.npz"))
+    kappa, Mb, ps = G["c4_kappa"], G["c4_Mbasis"], G["c4_ps"]
+    Qmax = int(G["c4_scal"][1])
+    geoms = [dict(kappa=kappa, Mbasis=Mb, Q=Qmax, dilation=1.0)]
+    qmax = nonconi.qmax_of(Qmax, 1.0)
+
+    def fake(geoms_, sub_ps, sub_pgeo, device=0, **kw):
+        Ms, Ks, qs, pid = [], [], [], []
+        for i, p in enumerate(sub_ps):
+            st, C, M, Kn, q = nonconi.ref_points(kappa, Mb, p, Qmax, qmax)
+            Ms.append(M); Ks.append(Kn); qs.append(q); pid.append(np.full(len(q), i))
+        M, Kn, q, pidx = np.vstack(Ms), np.vstack(Ks), np.concatenate(qs), np.concatenate(pid).astype(np.int64)
+        o = np.lexsort(tuple(Kn[:, j] for j in range(Kn.shape[1] - 1, -1, -1)) +
+                       tuple(M[:, j] for j in range(M.shape[1] - 1, -1, -1)) + (pidx,))
+        return M[o], Kn[o], q[o], pidx[o], np.zeros(len(sub_ps), np.int8), 0.01 * (device + 1), {}
+    monkeypatch.setattr(gpu, "zpm_batch_multi_ex", fake)
+    got = multi.zpm_batch_devices(geoms, ps, np.zeros(len(ps), np.int32), devices=[0, 1, 2], chunk=16)
+    one = fake(geoms, ps, np.zeros(len(ps), np.int32))
+    for a, b in zip(got[:5], one[:5]):
+        np.testing.assert_array_equal(a, b)
+    assert len(got[2]) > 100 and got[5] > 0
