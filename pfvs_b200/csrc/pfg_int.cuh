@@ -62,6 +62,10 @@ PFG_HD bool sub_ovf(i128 a, i128 b, i128 *r)
 // 2^64 and |a b| = hi(u) x 2^64 + lo(u) x for the other factor u.
 PFG_HD bool mul_ovf(i128 a, i128 b, i128 *r)
 {
+    // both int64 values (the usual case): one 64 x 64 -> 128-bit product, which
+    // always fits (|a b| <= 2^126), instead of a full 128 x 128-bit multiply
+    const int64_t a64 = (int64_t)a, b64 = (int64_t)b;
+    if ((i128)a64 == a && (i128)b64 == b) { *r = (i128)a64 * (i128)b64; return false; }
     u128 ua = uabs(a), ub = uabs(b);
     const u128 lim = (u128)1 << 63;
     if (ua < lim && ub < lim) { *r = a * b; return false; }
