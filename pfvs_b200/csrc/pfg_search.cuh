@@ -96,6 +96,14 @@ __device__ __forceinline__ i128 shfl128(i128 x, int src)
 __device__ __forceinline__ u128 shflu128(u128 x, int src) { return (u128)shfl128((i128)x, src); }
 __device__ __forceinline__ i128 warp_sum128(i128 x)
 {
+    // every lane's term below 2^58 in magnitude (the usual case): the sum of 32
+    // of them fits int64, so one 64-bit shuffle a round instead of two
+    const int64_t lo64 = (int64_t)x;
+    if (__all_sync(FULL, (i128)lo64 == x && lo64 < (1ll << 58) && lo64 > -(1ll << 58))) {
+        long long t = lo64;
+        for (int o = 16; o; o >>= 1) t += __shfl_xor_sync(FULL, t, o);
+        return (i128)t;
+    }
     for (int o = 16; o; o >>= 1) {
         long long lo = (long long)(uint64_t)x, hi = (long long)(x >> 64);
         lo = __shfl_xor_sync(FULL, lo, o);
@@ -534,7 +542,7 @@ __device__ int run_subtree(const SearchArgs &A, const Prob<R> &P, int pid, const
         }
         const int64_t cur = u_cur, hi = u_hi;
         // donate the top of the stack when other warps are idle
-        if (((++poll) & 4095) == 0 && (long long)(shfl(gtimer(), 0) - t0) > A.deadline_ns)
+        if (((++poll) & 1023) == 0 && (long long)(shfl(gtimer(), 0) - t0) > A.deadline_ns)
             return ST_WAIT;                       // (uniform: lane 0's clock)
         if (A.donate && (poll & 63) == 0) {
             int hungry = 0;
