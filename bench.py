@@ -50,19 +50,19 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 # Roofline of the dominant kernel, k_search<double, 1> (the persistent
-# FP64-pruned search, about 33 % of the launch list): scalar integer / FP64
+# FP64-pruned search, about 40 % of a timed call in the launch list): scalar integer / FP64
 # warp code, neither HBM- nor tensor-bound, so its ceiling is the
 # warp-instruction issue rate, 148 SMs x 4 schedulers x SM clock.  Per-unit
 # figures from one ncu --set full capture of the timed form's search on the
-# first 16,384 directions of this batch (20,582,107 nodes): executed warp
+# first 16,384 directions of this batch (20,582,108 nodes): executed warp
 # instructions and DRAM bytes per search node.
-SEARCH_INST_PER_NODE = 14_623_364_332 / 20_582_107
-SEARCH_DRAM_PER_NODE = (247_203_072 + 110_007_296) / 20_582_107
+SEARCH_INST_PER_NODE = 14_639_379_767 / 20_582_108
+SEARCH_DRAM_PER_NODE = (246_358_784 + 109_123_072) / 20_582_108
 # The setup's four phase kernels (k_setup<32, 0..3>) together, from the
 # same capture on the same 16,384 directions: per direction.
-SETUP_INST_PER_DIR = (3_753_500_525 + 6_287_646_566 + 255_177_793 + 1_542_075_343) / 16384
-SETUP_DRAM_PER_DIR = (112_741_632 + 255_599_360 + 223_871_488 + 14_464_000
-                      + 389_978_624 + 317_645_312 + 138_759_936 + 402_688) / 16384
+SETUP_INST_PER_DIR = (3_554_488_661 + 5_946_675_448 + 255_177_793 + 1_180_743_953) / 16384
+SETUP_DRAM_PER_DIR = (111_877_632 + 256_222_208 + 224_210_176 + 14_457_088
+                      + 390_921_472 + 315_255_040 + 139_578_880 + 386_816) / 16384
 N_SM, SCHEDULERS = 148, 4
 
 
