@@ -682,7 +682,8 @@ __device__ int run_subtree(const SearchArgs &A, const Prob<R> &P, int pid, const
         bool ok = pass;
         i128 q = 0;
         if (ok) {
-            q = A0 + (i128)2 * v * B0 + (i128)m00 * v * v;
+            // (|v| < 2^31: 2 v and v^2 are int64 values, so both products are 64 x 64-bit)
+            q = A0 + (i128)(2 * v) * (i128)B0 + (i128)m00 * (i128)(v * v);
             if (q > (i128)P.qmax) ok = false;
         }
         // Q g > q (coni: g = gcd(Kn[1:])) or Q g >= q (non-coni: g = gcd(Kn)) needs g exactly
