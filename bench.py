@@ -356,9 +356,10 @@ def pfv_rates(gpu, device, threads):
 
 
 def coni_zp_rates(device, threads):
-    """The exhaustive coniZp driver (pfvs_b200.coni: the dilation bound of
-    every direction on the device, then coniZpM at each direction's grid_up
-    bound with the device post-processing) on the dataset geometries, against
+    """The exhaustive coniZp driver (pfvs_b200.coni.coni_zp_multi: the dilation
+    bound of every direction on the device, then coniZpM at each direction's
+    grid_up bound with the device post-processing, all geometries' searches in
+    one call) on the dataset geometries, against
     the same plan on the host: the reference's C bound (coni_bound.h:255),
     the reference kernel at the same dilations and the oracle's restated
     post-processing, on `threads` threads.  And the bound alone at volume:
@@ -375,14 +376,13 @@ def coni_zp_rates(device, threads):
     n_dirs = sum(len(g["ps"]) for g in data)
 
     def device_run():
+        # every geometry's bounds, then all their searches in one device call (coni_zp_multi)
         t0 = time.perf_counter()
-        n_pfv, t_b, dil_max = 0, 0.0, 0
-        for g in data:
-            Ks, Ms, complete, info = coni.coni_zp(g["kappa"], g["Mbasis"], g["ps"], g["Q"], M0min=g["M0min"],
-                                                  device=device, return_info=True)
-            n_pfv += len(Ks)
-            t_b += info["seconds_bound"]
-            dil_max = max(dil_max, int(info["dilation"].max()))
+        res = coni.coni_zp_multi([dict(kappa=g["kappa"], Mbasis=g["Mbasis"], ps=g["ps"], Q=g["Q"], M0min=g["M0min"])
+                                  for g in data], device=device, return_info=True)
+        n_pfv = sum(len(r[0]) for r in res)
+        t_b = res[0][3]["seconds_bound"]
+        dil_max = max(int(r[3]["dilation"].max()) for r in res)
         return time.perf_counter() - t0, t_b, n_pfv, dil_max
     device_run()                                                    # (warm)
     runs = [device_run() for _ in range(3)]

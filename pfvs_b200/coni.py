@@ -71,45 +71,84 @@ def coni_zp(kappa, Mbasis, ps, Q, M0min=13, fallback_dilation=1, device=0, max_N
     a dict: keys (the p-vector of each PFV), status (the bound's), bceil,
     dilation (the searched one), pstat (the search's), seconds of each stage.
     """
+    item = dict(kappa=kappa, Mbasis=Mbasis, ps=ps, Q=Q, M0min=M0min)
+    return coni_zp_multi([item], fallback_dilation, device, max_N_pfvs, chunk, return_info)[0]
+
+
+def coni_zp_multi(items, fallback_dilation=1, device=0, max_N_pfvs=1_000_000_000, chunk=1 << 18,
+                  return_info=False):
+    """
+    coni_zp over several geometries at once: items is a list of dicts with
+    kappa, Mbasis, ps, Q and optionally M0min (13).  The bounds are computed
+    per geometry (one k_mu0 launch each); the searches of every geometry,
+    each distinct (geometry, dilation) pair a geometry entry, go to the
+    device together (one pipeline call per `chunk` p-vectors of the whole
+    list).  Returns, per item, what coni_zp returns for it.
+    """
     import time
     if fallback_dilation <= 0:
         raise ValueError(f"fallback_dilation must be > 0, got {fallback_dilation}.")
-    kappa = np.asarray(kappa, dtype=np.int64)
-    h = kappa.shape[0]
-    ps = np.atleast_2d(np.asarray(ps, dtype=np.int64))
-    if len(ps) == 0:
-        raise ValueError("ps must be non-empty.")
-    if ps.shape[1] != h - 1:
-        raise ValueError(f"ps must have h11 - 1 = {h - 1} columns (no coni entry), got {ps.shape[1]}")
-    n = len(ps)
-    p_full = np.hstack([np.zeros((n, 1), dtype=np.int64), ps])
     t0 = time.perf_counter()
-    bceil, bst = dilation.coni_dilation_bound_ceils(ps, kappa, Q, device=device, return_status=True)
+    per, P_all, key_all = [], [], []
+    for it in items:
+        kappa = np.asarray(it["kappa"], dtype=np.int64)
+        h = kappa.shape[0]
+        ps = np.atleast_2d(np.asarray(it["ps"], dtype=np.int64))
+        if len(ps) == 0:
+            raise ValueError("ps must be non-empty.")
+        if ps.shape[1] != h - 1:
+            raise ValueError(f"ps must have h11 - 1 = {h - 1} columns (no coni entry), got {ps.shape[1]}")
+        Q = int(it["Q"])
+        bceil, bst = dilation.coni_dilation_bound_ceils(ps, kappa, Q, device=device, return_status=True)
+        dil = route(bceil, fallback_dilation)
+        per.append(dict(kappa=kappa, h=h, Q=Q, M0min=it.get("M0min", 13), Mbasis=it["Mbasis"], n=len(ps),
+                        bceil=bceil, bst=bst, dil=dil, base=len(P_all)))
+        P_all.extend(np.hstack([np.zeros((len(ps), 1), dtype=np.int64), ps]))
+        key_all.extend((len(per) - 1, float(D)) for D in dil)
     t1 = time.perf_counter()
-    dil = route(bceil, fallback_dilation)
-    pieces_K, pieces_M, pieces_k = [], [], []
-    pstat = np.zeros(n, dtype=np.int8)
-    for lo in range(0, n, chunk):
-        idx = np.arange(lo, min(n, lo + chunk))
-        Ds, gi = np.unique(dil[idx], return_inverse=True)
-        geoms = [dict(kappa=kappa, Mbasis=Mbasis, Q=int(Q), dilation=float(D), M0min=M0min) for D in Ds]
-        K, M, pidx, pst, _, _ = gpu.coni_pfvs_multi(geoms, p_full[idx], gi.astype(np.int32), device=device)
-        counts = np.bincount(pidx, minlength=len(idx)) if len(pidx) else np.zeros(len(idx), dtype=np.int64)
+    pairs = sorted(set(key_all))
+    gid = {pk: g for g, pk in enumerate(pairs)}
+    geoms = [dict(kappa=per[k]["kappa"], Mbasis=per[k]["Mbasis"], Q=per[k]["Q"], dilation=D, M0min=per[k]["M0min"])
+             for k, D in pairs]
+    pgeo_all = np.array([gid[pk] for pk in key_all], dtype=np.int32)
+    N = len(P_all)
+    pstat = np.zeros(N, dtype=np.int8)
+    pieces = [([], [], []) for _ in per]
+    item_of = np.repeat(np.arange(len(per)), [it["n"] for it in per])
+    for lo in range(0, N, chunk):
+        hi = min(N, lo + chunk)
+        K, M, pidx, pst, _, _ = gpu.coni_pfvs_multi(geoms, P_all[lo:hi], pgeo_all[lo:hi], device=device)
+        counts = np.bincount(pidx, minlength=hi - lo) if len(pidx) else np.zeros(hi - lo, dtype=np.int64)
         pst = pst.copy()
         pst[(pst == 0) & (counts > max_N_pfvs)] = 1
-        pstat[idx] = pst
+        pstat[lo:hi] = pst
         keep = pst[pidx] == 0 if len(pidx) else np.zeros(0, dtype=bool)
-        pieces_K.append(np.asarray(K[keep][:, :h]))
-        pieces_M.append(np.asarray(M[keep][:, :h]))
-        pieces_k.append(idx[pidx[keep]])
+        gidx = lo + np.asarray(pidx)[keep]
+        Kk, Mk = np.asarray(K)[keep], np.asarray(M)[keep]
+        which = item_of[gidx] if len(gidx) else np.zeros(0, dtype=np.int64)
+        for k in np.unique(which):
+            sel = which == k
+            h = per[k]["h"]
+            pieces[k][0].append(Kk[sel][:, :h])
+            pieces[k][1].append(Mk[sel][:, :h])
+            pieces[k][2].append(gidx[sel] - per[k]["base"])
     t2 = time.perf_counter()
-    Ks, Ms, keys = _canonical(np.vstack(pieces_K), np.vstack(pieces_M), np.concatenate(pieces_k))
-    complete = (bceil > 0) & (pstat == 0)
-    if not return_info:
-        return Ks, Ms, complete
-    info = dict(keys=keys, status=bst, bceil=bceil, dilation=dil, pstat=pstat,
-                seconds_bound=t1 - t0, seconds_search=t2 - t1, seconds_total=time.perf_counter() - t0)
-    return Ks, Ms, complete, info
+    out = []
+    for k, it in enumerate(per):
+        h, n, base = it["h"], it["n"], it["base"]
+        Kp, Mp, kp = pieces[k]
+        Ks, Ms, keys = _canonical(np.vstack(Kp) if Kp else np.zeros((0, h), np.int64),
+                                  np.vstack(Mp) if Mp else np.zeros((0, h), np.int64),
+                                  np.concatenate(kp) if kp else np.zeros(0, np.int64))
+        ps_stat = pstat[base:base + n]
+        complete = (it["bceil"] > 0) & (ps_stat == 0)
+        if return_info:
+            info = dict(keys=keys, status=it["bst"], bceil=it["bceil"], dilation=it["dil"], pstat=ps_stat,
+                        seconds_bound=t1 - t0, seconds_search=t2 - t1, seconds_total=time.perf_counter() - t0)
+            out.append((Ks, Ms, complete, info))
+        else:
+            out.append((Ks, Ms, complete))
+    return out
 
 
 def coniZp(data, ps, Q=None, M0min=13, fallback_dilation=1, n_jobs=-1, device="auto", cost_model=None,

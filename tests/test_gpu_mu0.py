@@ -188,3 +188,17 @@ def test_search_past_the_bound_finds_nothing_more():
         at = _as_set(*_zpm_at(g, ps, b.astype(np.float64)))
         big = _as_set(*_zpm_at(g, ps, 2.0 * b + 20))
         assert at == big
+
+
+def test_coni_zp_multi_equals_per_geometry():
+    """All dataset geometries through coni_zp_multi (their searches in one
+    device call) give each geometry's coni_zp result."""
+    _need_gpu()
+    data = _dataset()
+    items = [dict(kappa=g["kappa"], Mbasis=g["Mbasis"], ps=g["ps"], Q=g["Q"], M0min=g["M0min"]) for g in data]
+    multi = coni.coni_zp_multi(items)
+    for g, (Ks, Ms, complete) in zip(data, multi):
+        one = coni.coni_zp(g["kappa"], g["Mbasis"], g["ps"], g["Q"], M0min=g["M0min"])
+        np.testing.assert_array_equal(Ks, one[0])
+        np.testing.assert_array_equal(Ms, one[1])
+        np.testing.assert_array_equal(complete, one[2])

@@ -225,3 +225,30 @@ def test_coni_zp_routing_and_canonical_order(monkeypatch):
     rows_ = np.hstack([keys[:, None], Ms, Ks])
     assert len(np.unique(rows_, axis=0)) == len(rows_)
     np.testing.assert_array_equal(np.unique(rows_, axis=0), rows_)
+
+
+def test_coni_zp_multi_equals_one_geometry_at_a_time(monkeypatch):
+    """coni_zp_multi (every geometry's searches in one device call) returns,
+    per geometry, what coni_zp returns for it alone."""
+    hs = {int(k): G[f"kappa{k}"].shape[0] for k in np.unique(G["gidx"])}
+    h = next(v for v in sorted(set(hs.values())) if sum(1 for x in hs.values() if x == v) >= 2)
+    ks = [k for k, v in hs.items() if v == h][:2]
+    items = []
+    for k in ks:
+        rows = [i for i in range(len(G["status"])) if int(G["gidx"][i]) == k][:3]
+        items.append(dict(kappa=G[f"kappa{k}"], Mbasis=np.eye(h, dtype=np.int64) * (k + 1),
+                          ps=np.array([G["p"][i][1:h] for i in rows]), Q=int(G["Q"][rows[0]]), M0min=13))
+
+    def zpm_points(p, D):
+        v = int(sum(p)) + int(D)
+        return [([0] + [v] * (h - 1), [1] + [2] * (h - 1)), ([0] * h, [int(D) % 7] + [1] * (h - 1))]
+    _fake_device(monkeypatch, zpm_points)
+    multi = coni.coni_zp_multi(items, return_info=True)
+    for it, (Ks, Ms, complete, info) in zip(items, multi):
+        one = coni.coni_zp(it["kappa"], it["Mbasis"], it["ps"], it["Q"], return_info=True)
+        np.testing.assert_array_equal(Ks, one[0])
+        np.testing.assert_array_equal(Ms, one[1])
+        np.testing.assert_array_equal(complete, one[2])
+        np.testing.assert_array_equal(info["keys"], one[3]["keys"])
+        np.testing.assert_array_equal(info["dilation"], one[3]["dilation"])
+        assert len(Ks) > 0
