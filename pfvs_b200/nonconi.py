@@ -27,7 +27,7 @@ import numpy as np
 
 from . import gpu, intlat
 
-PRIMES = (2147483647, 2147483629, 2147483587, 2147483579)
+PRIMES = (2147483647, 2147483629, 2147483587, 2147483579, 2147483563, 2147483549, 2147483543, 2147483497)
 STATUS_TEXT = {
     -2: "more than max_N_pfvs outputs; increase max_N_pfvs",
     -8: "lattice-point coordinates exceed int32",
@@ -114,7 +114,14 @@ def singular_mask(Ns):
             break
         nonzero[todo] = _det_mod(Ns[todo], p) != 0
     sing = ~nonzero
-    for i in np.flatnonzero(sing):
+    # det = 0 modulo every prime: det is a multiple of their product P, so it is 0
+    # when |det| < P, i.e. when Hadamard's bound (the product of the rows' lengths)
+    # is below P (log2 taken with a margin of two bits); otherwise exactly
+    rows = np.sum(np.asarray(Ns, dtype=np.float64) ** 2, axis=2)
+    with np.errstate(divide="ignore"):
+        log_hb = 0.5 * np.sum(np.log2(rows), axis=1)
+    log_p = sum(np.log2(float(p)) for p in PRIMES)
+    for i in np.flatnonzero(sing & ~(log_hb + 2.0 < log_p)):
         sing[i] = _det_exact(Ns[i]) == 0
     return sing
 
