@@ -16,9 +16,10 @@ typedef unsigned __int128 u128;
 #else
 #define PFG_NOINLINE __noinline__
 #endif
-// The LLL's inner steps (Gram-Schmidt row, size reduction, swap), inlined into
-// the one out-of-line LLL: called once per loop iteration, a call there costs
-// the saving and restoring of live registers through local memory.
+// The LLL's size reduction and swap, inlined into the one out-of-line LLL: called
+// once per loop iteration, a call there costs the saving and restoring of live
+// registers through local memory.  (Its Gram-Schmidt row stays out of line: it is
+// called from three places, and one copy of it keeps the loop's code smaller.)
 #ifndef PFG_LLL_INLINE
 #ifdef PFG_EMU
 #define PFG_LLL_INLINE

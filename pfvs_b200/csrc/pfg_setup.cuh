@@ -185,7 +185,7 @@ template <int N> struct Lll {
 // r_l (forward substitution by columns, lanes own rows); afterwards lane l
 // holds r_l, so mu_kl = r_l / bb_l and bb_k = G_kk - sum_l mu_kl r_l are
 // formed in parallel.
-template <int N> PFG_LLL_INLINE __device__ void lll_gs(LllMem<N> *S, int k, int lane)
+template <int N> PFG_NOINLINE __device__ void lll_gs(LllMem<N> *S, int k, int lane)
 {
     PFG_T0(t_gs);
     PFG_COUNT(12, 1);
