@@ -65,6 +65,11 @@ def _load():
         lib.ref_coni_mu0_batch.restype = None
         lib.ref_coni_mu0_batch.argtypes = [ctypes.c_int, _i64p, ctypes.c_int64, _i64p,
                                            ctypes.POINTER(ctypes.c_int32), _i64p, _i64p, _i64p]
+        lib.ref_coni_zpk_batch.restype = ctypes.c_long
+        lib.ref_coni_zpk_batch.argtypes = [
+            ctypes.c_int, _i64p, _i64p, _i64p, ctypes.c_long, ctypes.c_int64, ctypes.c_int64, ctypes.c_int64,
+            ctypes.c_long, ctypes.POINTER(_i64p), ctypes.POINTER(_i64p), ctypes.POINTER(_i64p),
+            ctypes.POINTER(_i64p), _i32p]
         lib.ref_lattice_build.restype = ctypes.c_int
         lib.ref_lattice_build.argtypes = [
             ctypes.c_int, _i64p, _i64p, _i64p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
@@ -239,3 +244,30 @@ def coni_mu0_batch(kappa, P):
     lib.ref_coni_mu0_batch(h, _p(kappa), n, _p(P), st.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)), _p(num),
                            _p(den), _p(K))
     return st[:n], num[:n], den[:n], K[:n]
+
+
+def coni_zpk_batch(kappa, Mbasis, ps, Q, M0min, D0, max_out=10**9):
+    """The reference's C coniZpK above D0 (coni_zpk.h:714) over the rows of ps
+    ((n, h), p[0] = 0): (M (N, h), Kn (N, h), q (N,), pidx (N,), status (n,)
+    int32), the points of the rows with status 0, in the reference's order."""
+    lib = _load()
+    kappa = np.ascontiguousarray(kappa, dtype=np.int64)
+    Mbasis = np.ascontiguousarray(Mbasis, dtype=np.int64)
+    h = Mbasis.shape[0]
+    ps = np.ascontiguousarray(np.atleast_2d(ps), dtype=np.int64).reshape(-1, h)
+    n = len(ps)
+    st = np.zeros(max(n, 1), np.int32)
+    Mp, Kp, qp, pp = _i64p(), _i64p(), _i64p(), _i64p()
+    N = lib.ref_coni_zpk_batch(h, _p(kappa), _p(Mbasis), _p(ps), n, int(Q), int(M0min), int(D0), int(max_out),
+                               ctypes.byref(Mp), ctypes.byref(Kp), ctypes.byref(qp), ctypes.byref(pp),
+                               st.ctypes.data_as(_i32p))
+    try:
+        M = np.ctypeslib.as_array(Mp, shape=(N, h)).copy() if N else np.zeros((0, h), np.int64)
+        Kn = np.ctypeslib.as_array(Kp, shape=(N, h)).copy() if N else np.zeros((0, h), np.int64)
+        q = np.ctypeslib.as_array(qp, shape=(N,)).copy() if N else np.zeros(0, np.int64)
+        pidx = np.ctypeslib.as_array(pp, shape=(N,)).copy() if N else np.zeros(0, np.int64)
+    finally:
+        for a in (Mp, Kp, qp, pp):
+            if a:
+                lib.ref_free(ctypes.cast(a, ctypes.c_void_p))
+    return M, Kn, q, pidx, st[:n]

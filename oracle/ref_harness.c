@@ -304,3 +304,25 @@ void ref_coni_mu0_batch(int h, const int64_t *kappa, int64_t n, const int64_t *P
     for (int64_t i = 0; i < n; ++i)
         st[i] = cb_coni_mu0(h, kappa, P + i * (h - 1), num + i, den + i, K + i * (h - 1));
 }
+
+/* The reference's coniZpK above D0 (pfvs/fp_kernel/coni_zpk.h:714, czk_batch,
+ * as its _coni_zpk_batch binding calls it, fp_kernel.pyx:434): for the n rows
+ * of ps ((n, h), p[0] = 0), the lattice points (M, Kn rows of h; q; pidx) and
+ * a status per row (points kept only where it is 0).  The arrays are
+ * malloc'd here (ref_free); returns the number of points. */
+#include "coni_zpk.h"
+long ref_coni_zpk_batch(int h, const int64_t *kappa, const int64_t *Mbasis, const int64_t *ps, long n, int64_t Q,
+                        int64_t M0min, int64_t D0, long max_out, int64_t **M, int64_t **Kn, int64_t **q,
+                        int64_t **pidx, int32_t *status)
+{
+    czk_points P;
+    memset(&P, 0, sizeof P);
+    int *st = (int *)malloc(sizeof(int) * (n ? n : 1));
+    for (long i = 0; i < n; ++i) st[i] = -20;
+    if (n && h >= 3 && h <= CZK_MAX_H11) czk_batch(h, kappa, Mbasis, ps, n, Q, M0min, D0, max_out, &P, st);
+    for (long i = 0; i < n; ++i) status[i] = st[i];
+    free(st);
+    *M = P.M; *Kn = P.Kn; *q = P.q; *pidx = P.pidx;
+    return P.n;
+}
+

@@ -10,7 +10,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB = os.path.join(HERE, "_build", "libpfvs_emu.so")
 SRCS = [os.path.join(HERE, f) for f in ("emu_driver.cpp", "warp_emu.h")] + [
     os.path.join(HERE, "..", "..", "pfvs_b200", "csrc", f) for f in
-    ("pfg_int.cuh", "pfg_types.cuh", "pfg_setup.cuh", "pfg_search.cuh", "pfg_out.cuh", "pfg_mu0.cuh")] + [
+    ("pfg_int.cuh", "pfg_types.cuh", "pfg_setup.cuh", "pfg_search.cuh", "pfg_out.cuh", "pfg_mu0.cuh", "pfg_zpk.cuh")] + [
     os.path.join(HERE, "..", "..", "include", "pfvs_gpu.h")]
 _lib = None
 
@@ -120,3 +120,32 @@ def coni_mu0_batch(kappa, p_r):
     lib.emu_coni_mu0_batch(h, kappa.ctypes.data_as(i64p), n, p_r.ctypes.data_as(i64p), st.ctypes.data_as(i32p),
                            num.ctypes.data_as(i64p), den.ctypes.data_as(i64p), K.ctypes.data_as(i64p))
     return st[:n], num[:n], den[:n], K[:n]
+
+
+def coni_zpk_batch(kappa, Mbasis, ps, Q, M0min, D0, max_out=10**9, budget=10**9):
+    """The device's coniZpK above D0 on the emulated warp: (M (N, h), Kn, q,
+    pidx, status) for the rows of ps ((n, h), p[0] = 0); points of every row
+    (the caller keeps those whose row has status 0)."""
+    lib = _load()
+    i64p, i32p = ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int32)
+    lib.emu_coni_zpk_batch.restype = ctypes.c_longlong
+    lib.emu_coni_zpk_batch.argtypes = [ctypes.c_int, i64p, i64p, i64p, ctypes.c_int64, ctypes.c_int64,
+                                       ctypes.c_int64, ctypes.c_int64, ctypes.c_int64, ctypes.c_longlong,
+                                       ctypes.c_ulonglong, i64p, i64p, i64p, i64p, i32p]
+    kappa = np.ascontiguousarray(kappa, dtype=np.int64)
+    Mbasis = np.ascontiguousarray(Mbasis, dtype=np.int64)
+    h = Mbasis.shape[0]
+    ps = np.ascontiguousarray(np.atleast_2d(ps), dtype=np.int64).reshape(-1, h)
+    n = len(ps)
+    st = np.zeros(max(n, 1), np.int32)
+    cap = 1024
+    while True:
+        M, Kn = np.zeros((cap, 64), np.int64), np.zeros((cap, 64), np.int64)
+        q, pidx = np.zeros(cap, np.int64), np.zeros(cap, np.int64)
+        N = lib.emu_coni_zpk_batch(h, kappa.ctypes.data_as(i64p), Mbasis.ctypes.data_as(i64p),
+                                   ps.ctypes.data_as(i64p), n, int(Q), int(M0min), int(D0), int(max_out),
+                                   int(budget), cap, M.ctypes.data_as(i64p), Kn.ctypes.data_as(i64p),
+                                   q.ctypes.data_as(i64p), pidx.ctypes.data_as(i64p), st.ctypes.data_as(i32p))
+        if N <= cap:
+            return M[:N, :h], Kn[:N, :h], q[:N], pidx[:N], st[:n]
+        cap = N

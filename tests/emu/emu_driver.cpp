@@ -21,6 +21,7 @@
 #include "../../pfvs_b200/csrc/pfg_search.cuh"
 #include "../../pfvs_b200/csrc/pfg_out.cuh"
 #include "../../pfvs_b200/csrc/pfg_mu0.cuh"
+#include "../../pfvs_b200/csrc/pfg_zpk.cuh"
 
 using namespace pfg;
 
@@ -229,4 +230,22 @@ extern "C" int emu_coni_mu0_batch(int h, const int64_t *kappa, int64_t n_p, cons
     Mu0Args A{h, kappa, p_r, (int)n_p, &next, scr.data(), status, num, den, K, 20000000ll};
     emu_run_warp(0, 0, 32, 1, [&] { k_mu0(A); });
     return 0;
+}
+
+
+// The device's coniZpK above D0 (pfg_zpk.cuh, k_zpk) on one emulated warp:
+// the points (rows of MH) into the caller's arrays of cap rows; returns the
+// number of points emitted (more than cap: call again with room for them).
+extern "C" long long emu_coni_zpk_batch(int h, const int64_t *kappa, const int64_t *Mbasis, const int64_t *ps,
+                                        int64_t n_p, int64_t Q, int64_t M0min, int64_t D0, int64_t max_out,
+                                        long long budget, unsigned long long cap, int64_t *M, int64_t *Kn,
+                                        int64_t *q, int64_t *pidx, int32_t *status)
+{
+    std::vector<ZpkScratch> scr(1);
+    unsigned next = 0;
+    unsigned long long count = 0;
+    ZpkArgs A{h, kappa, Mbasis, ps, (int)n_p, Q, M0min, D0, max_out, &next, scr.data(), status, &count, cap,
+              M, Kn, q, pidx, budget};
+    emu_run_warp(0, 0, 32, 1, [&] { k_zpk(A); });
+    return (long long)count;
 }
