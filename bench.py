@@ -443,6 +443,59 @@ def coni_zp_rates(device, threads):
     return out
 
 
+def zpk_rates(device, threads):
+    """coniZpK above D0 (pfg_coni_zpk_batch; the reference runs it on the CPU
+    only: coni_zpk.h:714 behind coniZpK) on the dataset geometries' 10,399
+    directions at D0 = 20 and 150: the kernel's device time and the whole
+    call, points/s and directions/s, and the PFVs through pfvs_b200.zpk; against
+    the reference's own C kernel (oracle/_ref) over the same directions on
+    `threads` threads."""
+    import concurrent.futures as cf
+    from oracle import ref
+    from pfvs_b200 import gpu, zpk
+    G = np.load(os.path.join(ROOT, "tests", "golden", "dataset_pfvs.npz"))
+    data = []
+    for k in range(int(G["n_geometries"][0])):
+        h, Q, m0 = (int(x) for x in G[f"g{k}_scal"])
+        data.append((G[f"g{k}_kappa"], G[f"g{k}_Mbasis"], G[f"g{k}_ps"], Q, m0))
+    n_dirs = sum(len(g[2]) for g in data)
+    out = {"workload": f"{len(data)} reference dataset geometries (h11 3..9), {n_dirs} p-vectors, the points and "
+                       f"PFVs of dilation above D0"}
+    for D0 in (20, 150):
+        for g in data[:2]:
+            gpu.coni_zpk_points(g[0], g[1], g[2], g[3], g[4], D0, device=device)     # (warm)
+        best = None
+        for _ in range(2):
+            t0 = time.perf_counter()
+            dev = pts = bad = 0
+            for g in data:
+                M, Kn, q, pidx, st, secs = gpu.coni_zpk_points(g[0], g[1], g[2], g[3], g[4], D0, device=device)
+                dev += secs
+                pts += len(q)
+                bad += int(np.sum(st != 0))
+            wall = time.perf_counter() - t0
+            if best is None or wall < best[0]:
+                best = (wall, dev, pts, bad)
+        t0 = time.perf_counter()
+        n_pfv = sum(len(zpk.coni_zpk(g[0], g[1], g[2][:, 1:], g[3], D0, M0min=g[4], device=device)[2]) for g in data)
+        pfv_wall = time.perf_counter() - t0
+        ent = {"points": int(best[2]), "not_decided": int(best[3]), "device_kernel_s": best[1], "wall_s": best[0],
+               "directions_per_s": n_dirs / best[0], "pfvs": int(n_pfv), "pfvs_wall_s": pfv_wall}
+        if ref.available():
+            jobs = [(g, c) for g in data for c in np.array_split(g[2], max(1, min(4 * threads, len(g[2]) // 8)))]
+            t1 = time.perf_counter()
+            with cf.ThreadPoolExecutor(threads) as ex:
+                parts = list(ex.map(lambda j: ref.coni_zpk_batch(j[0][0], j[0][1], j[1], j[0][3], j[0][4], D0),
+                                    sorted(jobs, key=lambda j: -len(j[1]) * j[0][0].shape[0] ** 3)))
+            dt = time.perf_counter() - t1
+            ent["cpu_reference"] = {"points": int(sum(len(x[2]) for x in parts)), "wall_s": dt,
+                                    "directions_per_s": n_dirs / dt, "threads": threads,
+                                    "what": "oracle/_ref: the reference's czk_batch (ctypes, the GIL released)"}
+            ent["device_vs_cpu_reference"] = dt / best[0]
+        out[f"D0={D0}"] = ent
+    return out
+
+
 def nonconi_rates(device, threads):
     """Non-coni ZpM (pfg_zpm_batch; the reference runs it on the CPU only) on
     the reference's non-coni Manwe test geometry (tests/golden/nonconi.npz):
@@ -698,6 +751,7 @@ def main():
             pfv["dataset"] = pfv_rates(gpu, device, threads)
             pfv["coni_zp"] = coni_zp_rates(device, threads)
             pfv["nonconi_zpm"] = nonconi_rates(device, threads)
+            pfv["coni_zpk"] = zpk_rates(device, threads)
     # roofline of the search kernel: executed warp instructions per launch (ncu
     # per-node figure x the launch's nodes) over its CUDA-event time (the
     # search stage: k_flip, a few microseconds, then k_search<double, 1>); the

@@ -191,6 +191,36 @@ int pfg_zpm_batch(const pfg_input *in, const pfg_options *opt, pfg_output *out, 
 int pfg_coni_mu0_batch(int h, const int64_t *kappa, int64_t n_p, const int64_t *p_r, int device,
                        int32_t *status, int64_t *mu_num, int64_t *mu_den, int64_t *K, char *err);
 
+/* coniZpK above D0 on the device (the reference computes it on the CPU:
+ * pfvs/fp_kernel/coni_zpk.h:714 czk_batch, bound by _coni_zpk_batch,
+ * pfvs/fp_kernel/fp_kernel.pyx:434, called by coniZpK, pfvs/coni.py:554):
+ * for each coni p-vector (rows of ps, (n_p, h) row-major, p[0] = 0) the
+ * lattice points c of its coni PFVs with dilation > D0, as M = Binter c,
+ * Kn = (Z Binter) c (rows of pfg_max_h11(), first h entries valid), q =
+ * c^T mat c and pidx -- the format of pfg_coni_batch -- and per p-vector a
+ * status into `status` ((n_p,)): 0 done; 1 no ZpK for the direction (s >= 0,
+ * A_rr singular, or S not positive definite on the lattice orthogonal to
+ * p); < 0 not decided here (a value beyond int128 / int64, an
+ * ill-conditioned form, more than max_out points, the search's step
+ * budget), the reference's codes where it has the same failure.  Points of
+ * a p-vector with a nonzero status are not returned (out->pstat stays
+ * NULL).  3 <= h <= 32 (the reference's C path: h <= 20).  Returns 0, or 1
+ * with out->err set; free with pfg_output_free. */
+int pfg_coni_zpk_batch(int h, const int64_t *kappa, const int64_t *Mbasis, int64_t n_p, const int64_t *ps,
+                       int64_t Q, int64_t M0min, int64_t D0, int64_t max_out, int device,
+                       pfg_output *out, int32_t *status);
+
+/* The same followed by coniZpM's post-processing on the device (as
+ * pfg_coni_pfvs; coniZpK applies the same _pfvs_from_points to its points,
+ * pfvs/coni.py:613): the PFVs (K, M, pidx) of the points, n_points the
+ * points they came from; pstat stays NULL (statuses into `status`).  The
+ * PFVs are not yet filtered by dilation > D0 (the reference filters after
+ * the post-processing, pfvs/coni.py:629-631).  M0min must be > 0.  Returns
+ * 0, or 1 with out->err set; free with pfg_pfv_output_free. */
+int pfg_coni_zpk_pfvs(int h, const int64_t *kappa, const int64_t *Mbasis, int64_t n_p, const int64_t *ps,
+                      int64_t Q, int64_t M0min, int64_t D0, int64_t max_out, int device,
+                      pfg_pfv_output *out, int32_t *status);
+
 /* Test hook (no counterpart in the reference): the k-th device allocation
  * this library makes from now on (k >= 1) fails once with
  * cudaErrorMemoryAllocation, without allocating, so that tests can drive the

@@ -11,7 +11,7 @@ SRCS = [os.path.join(HERE, "csrc", "pfg_abi.cu"), os.path.join(HERE, "csrc", "pf
 OUT = os.path.join(HERE, "fp_kernel", "libpfvs_gpu.so")
 DEPS = [os.path.join(HERE, "csrc", f) for f in
         ("pfg_abi.cu", "pfg_static.cu", "pfg_int.cuh", "pfg_types.cuh", "pfg_setup.cuh",
-         "pfg_search.cuh", "pfg_out.cuh", "pfg_pfv.cuh", "pfg_mu0.cuh")] + [os.path.join(HERE, "..", "include", "pfvs_gpu.h")]
+         "pfg_search.cuh", "pfg_out.cuh", "pfg_pfv.cuh", "pfg_mu0.cuh", "pfg_zpk.cuh")] + [os.path.join(HERE, "..", "include", "pfvs_gpu.h")]
 
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
               "-shared", "-Xcompiler", "-fPIC"]

@@ -33,6 +33,7 @@
 #include "pfg_out.cuh"
 #include "pfg_pfv.cuh"
 #include "pfg_mu0.cuh"
+#include "pfg_zpk.cuh"
 
 using namespace pfg;
 
@@ -62,7 +63,8 @@ enum {
     W_CTL, W_ITEMS, W_READY, W_HDR, W_COORDS, W_DIRNODES, W_DIRPASS,
     W_KEYS, W_COUNT, W_FILL, W_SEG, W_IDX, W_CSEG, W_SUM, W_PERM, W_PERM2, W_SIDX, W_PCNT, W_PKG, W_PEPT, W_PEG, W_PEK0, W_PEORD, W_PNONS, W_PKEEP,
     W_PERR, W_PSORT, W_PK, W_PM, W_PP, W_PRIMES, W_OM, W_OK, W_OQ, W_OP, W_OM2, W_OK2, W_OQ2, W_OP2, W_RETRY,
-    W_ROWS, W_MU_K, W_MU_P, W_MU_ST, W_MU_NUM, W_MU_DEN, W_MU_KO, W_MU_SCR, W_MU_CTR, W_N
+    W_ROWS, W_MU_K, W_MU_P, W_MU_ST, W_MU_NUM, W_MU_DEN, W_MU_KO, W_MU_SCR, W_MU_CTR,
+    W_ZK_MB, W_ZK_PS, W_ZK_SCR, W_ZK_CTR, W_ZK_ST, W_ZK_M, W_ZK_K, W_ZK_Q, W_ZK_P, W_N
 };
 
 struct Workspace {
@@ -332,6 +334,84 @@ extern "C" void pfg_debug_fail_alloc(int k) { g_fail_alloc.store(k > 0 ? k : 0);
 extern "C" int pfg_coni_batch(const pfg_input *in, pfg_output *out)
 {
     return pfg_coni_batch_ex(in, nullptr, out, nullptr, nullptr);
+}
+
+// Lattice points -> coni PFVs on the device (pfg_pfv.cuh) for n_out points in
+// device memory (rows of MH, pidx from pid_base; dirs / geo / kappa as the
+// setup wrote them): the PFVs are appended to pfv as one pinned chunk.
+// Returns 0, 1 with err set, or 2 when a device allocation ran out of memory
+// (err set too; the caller may retry with a smaller batch).
+static int pfv_stage(Workspace &W, int nsm, const Dir *ddirs, const Geo *dgeo, const int64_t *dkappa,
+                     const int64_t *oM, const int64_t *oK, const int64_t *oq, const int64_t *op,
+                     unsigned long long n_out, int64_t pid_base, int hmax2, PfvSink *pfv, int64_t &launches,
+                     char *err)
+{
+    cudaError_t e;
+#define PCK(x) do { e = (x); if (e != cudaSuccess) { snprintf(err, 256, "%s (%s:%d)", cudaGetErrorString(e), \
+    __FILE__, __LINE__); return 1; } } while (0)
+#define PWS(ptr, slot, bytes) do { e = ws_get(W, slot, (size_t)(bytes), (void **)&(ptr)); \
+    if (e != cudaSuccess) { snprintf(err, 256, "%s (%s:%d)", cudaGetErrorString(e), __FILE__, __LINE__); \
+    return e == cudaErrorMemoryAllocation ? 2 : 1; } } while (0)
+    pfv->n_points += (int64_t)n_out;
+    unsigned long long *pcnt, *pkeep; uint64_t *pkg; unsigned *pept, *peord, *psort;
+    int64_t *peg, *pek0; int *pnons, *perr; uint32_t *dprimes;
+    PWS(pcnt, W_PCNT, (n_out + 1) * 8);
+    PWS(pkg, W_PKG, n_out * 8);
+    PWS(pnons, W_PNONS, n_out * 4);
+    PWS(perr, W_PERR, 64);
+    PWS(dprimes, W_PRIMES, primes31().size() * 4);
+    PCK(cudaMemset(perr, 0, 64));
+    PCK(cudaMemcpy(dprimes, primes31().data(), primes31().size() * 4, cudaMemcpyHostToDevice));
+    PfvArgs PA{ddirs, dgeo, dkappa, oM, oK, oq, op, n_out, pid_base, pcnt, pkg, nullptr, nullptr, nullptr,
+               nullptr, pnons, nullptr, perr, dprimes, (int)primes31().size(), hmax2 - 1};
+    k_pfv_count<<<nsm * 4, 256>>>(PA); ++launches;
+    k_scan64<<<1, 1024>>>(pcnt, n_out); ++launches;
+    unsigned long long n_e = 0;
+    PCK(cudaMemcpy(&n_e, pcnt + n_out, 8, cudaMemcpyDeviceToHost));
+    unsigned long long n_pfv = 0;
+    if (n_e) {
+        unsigned np2 = 1;
+        while (np2 < n_e) np2 <<= 1;
+        PWS(pept, W_PEPT, n_e * 4);
+        PWS(peg, W_PEG, n_e * 8);
+        PWS(pek0, W_PEK0, n_e * 8);
+        PWS(peord, W_PEORD, n_e * 4);
+        PWS(pkeep, W_PKEEP, (n_e + 1) * 8);
+        PWS(psort, W_PSORT, (size_t)np2 * 4);
+        PA.e_pt = pept; PA.e_g = peg; PA.e_K0 = pek0; PA.e_ord = peord; PA.keep = pkeep;
+        k_pfv_fill<<<nsm * 4, 256>>>(PA); ++launches;
+        k_pfv_sort<<<1, 1024>>>(PA, n_e, np2, psort); ++launches;
+        k_pfv_det<<<(int)std::min<unsigned long long>(n_out, (unsigned long long)nsm * 32), 32,
+                    (size_t)(hmax2 - 1) * (hmax2 - 1) * 12>>>(PA); ++launches;
+        k_pfv_keep<<<nsm * 4, 256>>>(PA, n_e); ++launches;
+        k_scan64<<<1, 1024>>>(pkeep, n_e); ++launches;
+        PCK(cudaGetLastError());
+        PCK(cudaMemcpy(&n_pfv, pkeep + n_e, 8, cudaMemcpyDeviceToHost));
+    }
+    int herr[3] = {0, 0, 0};
+    if (n_pfv) {
+        int64_t *pK, *pM, *pP;
+        PWS(pK, W_PK, n_pfv * MH * 8);
+        PWS(pM, W_PM, n_pfv * MH * 8);
+        PWS(pP, W_PP, n_pfv * 8);
+        k_pfv_rows<<<nsm * 8, 256>>>(PA, n_e, pK, pM, pP); ++launches;
+        PCK(cudaGetLastError());
+        PfvChunk c{(int64_t *)pinned_get(n_pfv * MH * 8), (int64_t *)pinned_get(n_pfv * MH * 8),
+                   (int64_t *)pinned_get(n_pfv * 8), (size_t)n_pfv};
+        pfv->chunks.push_back(c);
+        if (!c.K || !c.M || !c.pidx) { snprintf(err, 256, "out of pinned host memory"); return 1; }
+        PCK(cudaMemcpy(c.K, pK, n_pfv * MH * 8, cudaMemcpyDeviceToHost));
+        PCK(cudaMemcpy(c.M, pM, n_pfv * MH * 8, cudaMemcpyDeviceToHost));
+        PCK(cudaMemcpy(c.pidx, pP, n_pfv * 8, cudaMemcpyDeviceToHost));
+    }
+    PCK(cudaMemcpy(herr, perr, sizeof herr, cudaMemcpyDeviceToHost));
+    if (herr[0]) { snprintf(err, 256, "Tadpole violation: -dot(K,M) > Q"); return 1; }
+    if (herr[1] == 2) { snprintf(err, 256, "determinant test: more primes needed than provided"); return 1; }
+    if (herr[1]) { snprintf(err, 256, "PFV entries beyond int64"); return 1; }
+    if (herr[2]) { snprintf(err, 256, "a point expands over more than 2^22 values of g"); return 1; }
+    return 0;
+#undef PCK
+#undef PWS
 }
 
 // The pipeline over all batches: points into `out`, or, with `pfv`, the
@@ -705,65 +785,12 @@ static int coni_run(const pfg_input *in, const pfg_options *opt_in, pfg_output *
             }
             if (pfv && n_out) {
                 // ---- points -> PFVs (on the device) ----
-                pfv->n_points += (int64_t)n_out;
-                unsigned long long *pcnt, *pkeep; uint64_t *pkg; unsigned *pept, *peord, *psort;
-                int64_t *peg, *pek0; int *pnons, *perr; uint32_t *dprimes;
-                WSB(pcnt, W_PCNT, (n_out + 1) * 8);
-                WSB(pkg, W_PKG, n_out * 8);
-                WSB(pnons, W_PNONS, n_out * 4);
-                WSB(perr, W_PERR, 64);
-                WSB(dprimes, W_PRIMES, primes31().size() * 4);
-                CK(cudaMemset(perr, 0, 64));
-                CK(cudaMemcpy(dprimes, primes31().data(), primes31().size() * 4, cudaMemcpyHostToDevice));
                 int hmax2 = 3;
                 for (int k = 0; k < nb; ++k) hmax2 = std::max(hmax2, geos[in->pgeo[off + k]].h);
-                PfvArgs PA{ddirs, dgeo, dkappa, oM, oK, oq, op, n_out, off, pcnt, pkg, nullptr, nullptr, nullptr,
-                           nullptr, pnons, nullptr, perr, dprimes, (int)primes31().size(), hmax2 - 1};
-                k_pfv_count<<<nsm * 4, 256>>>(PA); ++launches;
-                k_scan64<<<1, 1024>>>(pcnt, n_out); ++launches;
-                unsigned long long n_e = 0;
-                CK(cudaMemcpy(&n_e, pcnt + n_out, 8, cudaMemcpyDeviceToHost));
-                unsigned long long n_pfv = 0;
-                if (n_e) {
-                    unsigned np2 = 1;
-                    while (np2 < n_e) np2 <<= 1;
-                    WSB(pept, W_PEPT, n_e * 4);
-                    WSB(peg, W_PEG, n_e * 8);
-                    WSB(pek0, W_PEK0, n_e * 8);
-                    WSB(peord, W_PEORD, n_e * 4);
-                    WSB(pkeep, W_PKEEP, (n_e + 1) * 8);
-                    WSB(psort, W_PSORT, (size_t)np2 * 4);
-                    PA.e_pt = pept; PA.e_g = peg; PA.e_K0 = pek0; PA.e_ord = peord; PA.keep = pkeep;
-                    k_pfv_fill<<<nsm * 4, 256>>>(PA); ++launches;
-                    k_pfv_sort<<<1, 1024>>>(PA, n_e, np2, psort); ++launches;
-                    k_pfv_det<<<(int)std::min<unsigned long long>(n_out, (unsigned long long)nsm * 32), 32,
-                                (size_t)(hmax2 - 1) * (hmax2 - 1) * 12>>>(PA); ++launches;
-                    k_pfv_keep<<<nsm * 4, 256>>>(PA, n_e); ++launches;
-                    k_scan64<<<1, 1024>>>(pkeep, n_e); ++launches;
-                    CK(cudaGetLastError());
-                    CK(cudaMemcpy(&n_pfv, pkeep + n_e, 8, cudaMemcpyDeviceToHost));
-                }
-                int herr[3] = {0, 0, 0};
-                if (n_pfv) {
-                    int64_t *pK, *pM, *pP;
-                    WSB(pK, W_PK, n_pfv * MH * 8);
-                    WSB(pM, W_PM, n_pfv * MH * 8);
-                    WSB(pP, W_PP, n_pfv * 8);
-                    k_pfv_rows<<<nsm * 8, 256>>>(PA, n_e, pK, pM, pP); ++launches;
-                    CK(cudaGetLastError());
-                    PfvChunk c{(int64_t *)pinned_get(n_pfv * MH * 8), (int64_t *)pinned_get(n_pfv * MH * 8),
-                               (int64_t *)pinned_get(n_pfv * 8), (size_t)n_pfv};
-                    pfv->chunks.push_back(c);
-                    if (!c.K || !c.M || !c.pidx) { set_err(out, "out of pinned host memory"); rc = 1; goto fail; }
-                    CK(cudaMemcpy(c.K, pK, n_pfv * MH * 8, cudaMemcpyDeviceToHost));
-                    CK(cudaMemcpy(c.M, pM, n_pfv * MH * 8, cudaMemcpyDeviceToHost));
-                    CK(cudaMemcpy(c.pidx, pP, n_pfv * 8, cudaMemcpyDeviceToHost));
-                }
-                CK(cudaMemcpy(herr, perr, sizeof herr, cudaMemcpyDeviceToHost));
-                if (herr[0]) { set_err(out, "Tadpole violation: -dot(K,M) > Q"); rc = 1; goto fail; }
-                if (herr[1] == 2) { set_err(out, "determinant test: more primes needed than provided"); rc = 1; goto fail; }
-                if (herr[1]) { set_err(out, "PFV entries beyond int64"); rc = 1; goto fail; }
-                if (herr[2]) { set_err(out, "a point expands over more than 2^22 values of g"); rc = 1; goto fail; }
+                const int prc = pfv_stage(W, nsm, ddirs, dgeo, dkappa, oM, oK, oq, op, n_out, off, hmax2, pfv,
+                                          launches, out->err);
+                if (prc == 2 && nb > 1) { out->err[0] = 0; goto out_of_memory; }
+                if (prc) { rc = 1; goto fail; }
             }
             CK(cudaEventRecord(ev[4]));
             if (n_out && !pfv) {
@@ -1013,5 +1040,200 @@ mu_fail:
         cudaGetLastError();
         if (err) memcpy(err, msg, sizeof msg);
     }
+    return rc;
+}
+
+// ---------------------------------------------------------------------------
+// coniZpK above D0 (pfg_zpk.cuh)
+// ---------------------------------------------------------------------------
+namespace {
+
+constexpr long long ZPK_STEP_BUDGET = 100000000ll;  // search nodes + (j, M0) steps per direction
+
+struct EventPair {
+    cudaEvent_t a = nullptr, b = nullptr;
+    ~EventPair() { if (a) cudaEventDestroy(a); if (b) cudaEventDestroy(b); }
+};
+
+// k_zpk over the n_p directions; the points of the directions with status 0
+// into host rows (MH wide), the statuses into `status`.  kappa stays on the
+// device in W_MU_K (*dkappa).  Returns 0 or 1 with err set.
+int zpk_points(Workspace &W, int h, const int64_t *kappa, const int64_t *Mbasis, int64_t n_p, const int64_t *ps,
+               int64_t Q, int64_t M0min, int64_t D0, int64_t max_out, int device, int32_t *status,
+               std::vector<int64_t> &M, std::vector<int64_t> &Kn, std::vector<int64_t> &q, std::vector<int64_t> &pidx,
+               double &secs, int &nsm, int64_t **dkappa, char *err)
+{
+    cudaError_t e;
+#define ZCK(x) do { e = (x); if (e != cudaSuccess) { snprintf(err, 256, "%s (%s:%d)", cudaGetErrorString(e), \
+    __FILE__, __LINE__); return 1; } } while (0)
+    int bps = 0;
+    ZCK(cudaSetDevice(device));
+    ZCK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device));
+    ZCK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_zpk, 128, 0));
+    const int grid = (int)std::min<int64_t>((n_p + 3) / 4, (int64_t)nsm * std::max(1, std::min(bps, 4)));
+    int64_t *dk, *dmb, *dps, *dM, *dK, *dq, *dp; int32_t *dst; ZpkScratch *dscr; unsigned *dctr;
+    ZCK(ws_get(W, W_MU_K, (size_t)h * h * h * 8, (void **)&dk));
+    ZCK(ws_get(W, W_ZK_MB, (size_t)h * h * 8, (void **)&dmb));
+    ZCK(ws_get(W, W_ZK_PS, (size_t)n_p * h * 8, (void **)&dps));
+    ZCK(ws_get(W, W_ZK_ST, (size_t)n_p * 4, (void **)&dst));
+    ZCK(ws_get(W, W_ZK_SCR, (size_t)grid * 4 * sizeof(ZpkScratch), (void **)&dscr));
+    ZCK(ws_get(W, W_ZK_CTR, 64, (void **)&dctr));
+    ZCK(cudaMemcpy(dk, kappa, (size_t)h * h * h * 8, cudaMemcpyHostToDevice));
+    ZCK(cudaMemcpy(dmb, Mbasis, (size_t)h * h * 8, cudaMemcpyHostToDevice));
+    ZCK(cudaMemcpy(dps, ps, (size_t)n_p * h * 8, cudaMemcpyHostToDevice));
+    *dkappa = dk;
+    EventPair ev;
+    ZCK(cudaEventCreate(&ev.a));
+    ZCK(cudaEventCreate(&ev.b));
+    unsigned long long cap = std::max<unsigned long long>(1ull << 14, (unsigned long long)n_p * 8), count = 0;
+    for (int pass = 0; pass < 2; ++pass) {
+        ZCK(ws_get(W, W_ZK_M, cap * MH * 8, (void **)&dM));
+        ZCK(ws_get(W, W_ZK_K, cap * MH * 8, (void **)&dK));
+        ZCK(ws_get(W, W_ZK_Q, cap * 8, (void **)&dq));
+        ZCK(ws_get(W, W_ZK_P, cap * 8, (void **)&dp));
+        ZCK(cudaMemset(dctr, 0, 64));
+        ZpkArgs A{h, dk, dmb, dps, (int)n_p, Q, M0min, D0, max_out, dctr, dscr, dst,
+                  (unsigned long long *)(dctr + 2), cap, dM, dK, dq, dp, ZPK_STEP_BUDGET};
+        ZCK(cudaEventRecord(ev.a));
+        k_zpk<<<grid, 128>>>(A);
+        ZCK(cudaGetLastError());
+        ZCK(cudaEventRecord(ev.b));
+        ZCK(cudaMemcpy(&count, dctr + 2, 8, cudaMemcpyDeviceToHost));
+        if (count <= cap) break;
+        cap = count;                            // (the same points again, with room for all of them)
+    }
+    float ms = 0.f;
+    ZCK(cudaEventElapsedTime(&ms, ev.a, ev.b));
+    secs = ms * 1e-3;
+    ZCK(cudaMemcpy(status, dst, (size_t)n_p * 4, cudaMemcpyDeviceToHost));
+    std::vector<int64_t> aM(count * MH), aK(count * MH), aq(count), ap(count);
+    if (count) {
+        ZCK(cudaMemcpy(aM.data(), dM, count * MH * 8, cudaMemcpyDeviceToHost));
+        ZCK(cudaMemcpy(aK.data(), dK, count * MH * 8, cudaMemcpyDeviceToHost));
+        ZCK(cudaMemcpy(aq.data(), dq, count * 8, cudaMemcpyDeviceToHost));
+        ZCK(cudaMemcpy(ap.data(), dp, count * 8, cudaMemcpyDeviceToHost));
+    }
+    M.clear(); Kn.clear(); q.clear(); pidx.clear();
+    for (unsigned long long t = 0; t < count; ++t) {
+        if (status[ap[t]] != 0) continue;       // (a direction's points count only when it finished)
+        M.insert(M.end(), aM.begin() + t * MH, aM.begin() + (t + 1) * MH);
+        Kn.insert(Kn.end(), aK.begin() + t * MH, aK.begin() + (t + 1) * MH);
+        q.push_back(aq[t]);
+        pidx.push_back(ap[t]);
+    }
+    return 0;
+#undef ZCK
+}
+
+bool zpk_args_ok(int h, const int64_t *kappa, const int64_t *Mbasis, int64_t n_p, const int64_t *ps,
+                 const int32_t *status, char *err)
+{
+    if (h < 3 || h > ZPK_MAXH || n_p < 0 || n_p > INT32_MAX || (n_p && (!kappa || !Mbasis || !ps || !status))) {
+        snprintf(err, 256, "coniZpK: bad arguments (h11 = %d outside 3..%d, or null arrays)", h, ZPK_MAXH);
+        return false;
+    }
+    return true;
+}
+
+}  // namespace
+
+extern "C" int pfg_coni_zpk_batch(int h, const int64_t *kappa, const int64_t *Mbasis, int64_t n_p, const int64_t *ps,
+                                  int64_t Q, int64_t M0min, int64_t D0, int64_t max_out, int device,
+                                  pfg_output *out, int32_t *status)
+{
+    memset(out, 0, sizeof *out);
+    if (!zpk_args_ok(h, kappa, Mbasis, n_p, ps, status, out->err)) return 1;
+    if (n_p == 0) return 0;
+    Workspace &W = workspace(device);
+    std::lock_guard<std::mutex> lock(W.mu);
+    std::vector<int64_t> M, Kn, q, pidx;
+    int nsm = 148;
+    int64_t *dk = nullptr;
+    if (zpk_points(W, h, kappa, Mbasis, n_p, ps, Q, M0min, D0, max_out, device, status, M, Kn, q, pidx,
+                   out->seconds_gpu, nsm, &dk, out->err)) {
+        cudaGetLastError();
+        return 1;
+    }
+    const size_t n = q.size();
+    out->n = (int64_t)n;
+    out->M = (int64_t *)pinned_get(std::max<size_t>(n, 1) * MH * 8);
+    out->Kn = (int64_t *)pinned_get(std::max<size_t>(n, 1) * MH * 8);
+    out->q = (int64_t *)pinned_get(std::max<size_t>(n, 1) * 8);
+    out->pidx = (int64_t *)pinned_get(std::max<size_t>(n, 1) * 8);
+    if (!out->M || !out->Kn || !out->q || !out->pidx) {
+        snprintf(out->err, sizeof out->err, "out of pinned host memory");
+        pfg_output_free(out);
+        return 1;
+    }
+    if (n) {
+        memcpy(out->M, M.data(), n * MH * 8);
+        memcpy(out->Kn, Kn.data(), n * MH * 8);
+        memcpy(out->q, q.data(), n * 8);
+        memcpy(out->pidx, pidx.data(), n * 8);
+    }
+    return 0;
+}
+
+extern "C" int pfg_coni_zpk_pfvs(int h, const int64_t *kappa, const int64_t *Mbasis, int64_t n_p, const int64_t *ps,
+                                 int64_t Q, int64_t M0min, int64_t D0, int64_t max_out, int device,
+                                 pfg_pfv_output *out, int32_t *status)
+{
+    memset(out, 0, sizeof *out);
+    if (!zpk_args_ok(h, kappa, Mbasis, n_p, ps, status, out->err)) return 1;
+    if (M0min <= 0) { snprintf(out->err, sizeof out->err, "coniZpK requires M0min > 0"); return 1; }
+    if (n_p == 0) return 0;
+    Workspace &W = workspace(device);
+    std::lock_guard<std::mutex> lock(W.mu);
+    std::vector<int64_t> M, Kn, q, pidx;
+    int nsm = 148;
+    int64_t *dk = nullptr;
+    PfvSink sink;
+    int rc = 0;
+    if (zpk_points(W, h, kappa, Mbasis, n_p, ps, Q, M0min, D0, max_out, device, status, M, Kn, q, pidx,
+                   out->seconds_gpu, nsm, &dk, out->err)) {
+        cudaGetLastError();
+        return 1;
+    }
+    const size_t n = q.size();
+    out->n_points = 0;
+    if (n) {
+        cudaError_t e;
+        int64_t *dM, *dK, *dq, *dp, launches = 0;
+        Dir *ddirs; Geo *dgeo;
+        std::vector<Dir> dirs(n_p);
+        for (auto &D : dirs) { D = Dir{}; D.geo = 0; D.h = h; D.d = h - 1; }
+        Geo g{};
+        g.h = h; g.d = h - 1; g.coni = 1; g.Q = Q; g.linmin = M0min; g.koff = 0;
+#define ZCK2(x) do { e = (x); if (e != cudaSuccess) { snprintf(out->err, sizeof out->err, "%s (%s:%d)", \
+    cudaGetErrorString(e), __FILE__, __LINE__); rc = 1; goto zfail; } } while (0)
+        ZCK2(ws_get(W, W_OM, n * MH * 8, (void **)&dM));
+        ZCK2(ws_get(W, W_OK, n * MH * 8, (void **)&dK));
+        ZCK2(ws_get(W, W_OQ, n * 8, (void **)&dq));
+        ZCK2(ws_get(W, W_OP, n * 8, (void **)&dp));
+        ZCK2(ws_get(W, W_DIRS, (size_t)n_p * sizeof(Dir), (void **)&ddirs));
+        ZCK2(ws_get(W, W_GEO, sizeof(Geo), (void **)&dgeo));
+        ZCK2(cudaMemcpy(dM, M.data(), n * MH * 8, cudaMemcpyHostToDevice));
+        ZCK2(cudaMemcpy(dK, Kn.data(), n * MH * 8, cudaMemcpyHostToDevice));
+        ZCK2(cudaMemcpy(dq, q.data(), n * 8, cudaMemcpyHostToDevice));
+        ZCK2(cudaMemcpy(dp, pidx.data(), n * 8, cudaMemcpyHostToDevice));
+        ZCK2(cudaMemcpy(ddirs, dirs.data(), (size_t)n_p * sizeof(Dir), cudaMemcpyHostToDevice));
+        ZCK2(cudaMemcpy(dgeo, &g, sizeof(Geo), cudaMemcpyHostToDevice));
+        if (pfv_stage(W, nsm, ddirs, dgeo, dk, dM, dK, dq, dp, n, 0, h, &sink, launches, out->err)) { rc = 1; goto zfail; }
+#undef ZCK2
+    }
+    {
+        size_t np_ = 0;
+        for (auto &c : sink.chunks) np_ += c.n;
+        out->n = (int64_t)np_;
+        out->n_points = (int64_t)n;
+        if (sink.chunks.size() == 1) {
+            out->K = sink.chunks[0].K; out->M = sink.chunks[0].M; out->pidx = sink.chunks[0].pidx;
+            sink.chunks.clear();
+        }
+    }
+    return 0;
+zfail:
+    cudaGetLastError();
+    sink.release();
     return rc;
 }

@@ -120,6 +120,12 @@ def _load():
     lib.pfg_coni_mu0_batch.argtypes = [ctypes.c_int, _i64p, ctypes.c_int64, _i64p, ctypes.c_int, _i32p,
                                        _i64p, _i64p, _i64p, ctypes.c_char_p]
     lib.pfg_coni_mu0_batch.restype = ctypes.c_int
+    zpk_args = [ctypes.c_int, _i64p, _i64p, ctypes.c_int64, _i64p, ctypes.c_int64, ctypes.c_int64, ctypes.c_int64,
+                ctypes.c_int64, ctypes.c_int]
+    lib.pfg_coni_zpk_batch.argtypes = zpk_args + [ctypes.POINTER(_Output), _i32p]
+    lib.pfg_coni_zpk_batch.restype = ctypes.c_int
+    lib.pfg_coni_zpk_pfvs.argtypes = zpk_args + [ctypes.POINTER(_PfvOutput), _i32p]
+    lib.pfg_coni_zpk_pfvs.restype = ctypes.c_int
     _lib = lib
     return lib
 
@@ -442,3 +448,65 @@ def coni_batch(kappa, Mbasis, ps, Q, dilation, M0min, max_N_out, device=0):
         kept = ~np.isin(pidx, too_many)
         M, Kn, q, pidx = M[kept], Kn[kept], q[kept], pidx[kept]
     return M[:, :hh], Kn[:, :hh], q, pidx, pstat
+
+
+def _zpk_arrays(kappa, Mbasis, ps):
+    kappa = np.ascontiguousarray(kappa, dtype=np.int64)
+    Mbasis = np.ascontiguousarray(Mbasis, dtype=np.int64)
+    h = Mbasis.shape[0]
+    if kappa.shape != (h, h, h):
+        raise ValueError(f"kappa must be ({h}, {h}, {h}), got {kappa.shape}")
+    ps = np.ascontiguousarray(np.atleast_2d(ps), dtype=np.int64)
+    if ps.shape[1] != h:
+        raise ValueError(f"ps must have h11 = {h} columns (p[0] = 0), got {ps.shape[1]}")
+    return kappa, Mbasis, ps, h
+
+
+def coni_zpk_points(kappa, Mbasis, ps, Q, M0min, D0, max_out=10**9, device=0):
+    """
+    coniZpK above D0 on the device (pfg_coni_zpk_batch; the reference's
+    _coni_zpk_batch, pfvs/fp_kernel/fp_kernel.pyx:434): for each row p of ps
+    ((n, h11), p[0] = 0) the lattice points of its coni PFVs with dilation
+    > D0.  Returns (M (N, h11), Kn (N, h11), q (N,), pidx (N,), status (n,)
+    int32, seconds_gpu); points only of the rows with status 0.
+    """
+    lib = _require()
+    MH = lib.pfg_max_h11()
+    kappa, Mbasis, ps, h = _zpk_arrays(kappa, Mbasis, ps)
+    n = len(ps)
+    st = np.zeros(max(n, 1), np.int32)
+    out = _Output()
+    rc = lib.pfg_coni_zpk_batch(h, kappa.ctypes.data_as(_i64p), Mbasis.ctypes.data_as(_i64p), n,
+                                ps.ctypes.data_as(_i64p), int(Q), int(M0min), int(D0), int(max_out), int(device),
+                                ctypes.byref(out), st.ctypes.data_as(_i32p))
+    if rc != 0:
+        raise RuntimeError(f"coniZpK failed: {out.err.decode(errors='replace')}")
+    M, Kn, q, pidx, _, secs = _points(lib, out, 0, MH)
+    return M[:, :h].copy(), Kn[:, :h].copy(), q.copy(), pidx.copy(), st[:n], secs
+
+
+def coni_zpk_pfvs(kappa, Mbasis, ps, Q, M0min, D0, max_out=10**9, device=0):
+    """
+    coniZpK above D0 and coniZpM's post-processing, both on the device
+    (pfg_coni_zpk_pfvs): (Ks (N, h11), Ms, pidx, status (n,) int32,
+    n_points, seconds_gpu) -- the PFVs of the points, not yet filtered by
+    dilation > D0.
+    """
+    lib = _require()
+    MH = lib.pfg_max_h11()
+    kappa, Mbasis, ps, h = _zpk_arrays(kappa, Mbasis, ps)
+    n = len(ps)
+    st = np.zeros(max(n, 1), np.int32)
+    out = _PfvOutput()
+    rc = lib.pfg_coni_zpk_pfvs(h, kappa.ctypes.data_as(_i64p), Mbasis.ctypes.data_as(_i64p), n,
+                               ps.ctypes.data_as(_i64p), int(Q), int(M0min), int(D0), int(max_out), int(device),
+                               ctypes.byref(out), st.ctypes.data_as(_i32p))
+    if rc != 0:
+        raise RuntimeError(f"coniZpK failed: {out.err.decode(errors='replace')}")
+    owner = _PfvOwner(lib, out)
+    N = out.n
+    K, M = _view(owner, out.K, (N, MH)), _view(owner, out.M, (N, MH))
+    pidx = _view(owner, out.pidx, (N,))
+    res = (K[:, :h].copy(), M[:, :h].copy(), pidx.copy(), st[:n], int(out.n_points), out.seconds_gpu)
+    del owner
+    return res

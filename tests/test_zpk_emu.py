@@ -1,0 +1,103 @@
+"""
+The device's coniZpK above D0 (pfvs_b200/csrc/pfg_zpk.cuh, k_zpk) run on the
+CPU warp emulator (tests/emu), against the reference's own C kernel
+(czk_batch, pfvs/fp_kernel/coni_zpk.h:714) through the committed golden
+vectors (tests/golden/zpk.npz, made by tests/golden/make_zpk_golden.py):
+
+- on the 30 dataset geometries (h11 3..9), 8 directions each, D0 in
+  (20, 150): the same statuses and the same multiset of lattice points
+  (pidx, M, Kn, q), although the device's bases of the M-lattice and of
+  Lambda are its own (the points do not depend on them);
+- the argument and hypothesis failures: D0 < 1 or M0min < 1 (-100, as the
+  reference), h11 beyond the kernel (-20), and directions without a bound
+  (s > 0 or S not positive definite) status 1, as the reference's C code;
+- max_out: a direction with more points than max_out ends with -80 and
+  keeps none (the reference's rule).
+"""
+import os
+
+import numpy as np
+import pytest
+
+from conftest import ROOT
+from emu import emu
+
+Z = np.load(os.path.join(ROOT, "tests", "golden", "zpk.npz"))
+D = np.load(os.path.join(ROOT, "tests", "golden", "dataset_pfvs.npz"))
+N_GEO = len([k for k in D.files if k.endswith("_kappa")])
+
+
+def _rows(M, Kn, q, pidx, st):
+    ok = st[pidx] == 0 if len(pidx) else np.zeros(0, dtype=bool)
+    A = np.hstack([pidx[ok, None], M[ok], Kn[ok], q[ok, None]]).astype(np.int64)
+    return A[np.lexsort(A.T[::-1])] if len(A) else A.reshape(0, A.shape[1] if A.ndim == 2 else 0)
+
+
+def _geo(g):
+    h, Q, M0min = (int(x) for x in D[f"g{g}_scal"])
+    return D[f"g{g}_kappa"], D[f"g{g}_Mbasis"], Z[f"g{g}_ps"], h, Q, M0min
+
+
+@pytest.mark.parametrize("D0", [20, 150])
+def test_device_zpk_points_equal_the_reference(D0):
+    total = 0
+    for g in range(N_GEO):
+        kappa, Mb, ps, h, Q, M0min = _geo(g)
+        M, Kn, q, pidx, st = emu.coni_zpk_batch(kappa, Mb, ps, Q, M0min, D0)
+        np.testing.assert_array_equal(st, Z[f"g{g}_d{D0}_status"], err_msg=f"geometry {g}")
+        want = Z[f"g{g}_d{D0}_points"]
+        got = _rows(M, Kn, q, pidx, st)
+        assert got.shape[0] == want.shape[0], (g, D0)
+        if len(want):
+            np.testing.assert_array_equal(got, want, err_msg=f"geometry {g}")
+        total += len(want)
+    assert total > (1500 if D0 == 20 else 500)
+
+
+def test_device_zpk_argument_failures():
+    kappa, Mb, ps, h, Q, M0min = _geo(5)
+    for D0, m0 in ((0, M0min), (20, 0)):
+        M, Kn, q, pidx, st = emu.coni_zpk_batch(kappa, Mb, ps[:2], Q, m0, D0)
+        assert list(st) == [-100, -100]
+    M, Kn, q, pidx, st = emu.coni_zpk_batch(np.zeros((2, 2, 2), np.int64), np.eye(2, dtype=np.int64),
+                                            np.array([[0, 1]]), Q, M0min, 20)
+    assert list(st) == [-20]
+
+
+def test_device_zpk_max_out_drops_the_direction():
+    kappa, Mb, ps, h, Q, M0min = _geo(13)
+    pts = Z["g13_d20_points"]
+    per = np.bincount(pts[:, 0], minlength=len(ps))
+    assert per.max() > 3
+    M, Kn, q, pidx, st = emu.coni_zpk_batch(kappa, Mb, ps, Q, M0min, 20, max_out=3)
+    np.testing.assert_array_equal(st == -80, per > 3)
+    kept = _rows(M, Kn, q, pidx, st)
+    want = pts[np.isin(pts[:, 0], np.flatnonzero(per <= 3))]
+    np.testing.assert_array_equal(kept, want)
+
+
+def test_device_zpk_no_bound_directions_match_the_reference():
+    """Directions whose dilation bound has no value (mu0 status 1: s > 0 or
+    S not positive definite on Lambda) have no ZpK either: status 1, as the
+    reference's C code says for the same inputs."""
+    from oracle import ref
+    if not ref.available():
+        pytest.skip("the reference's C build (oracle/_ref) is not present")
+    G = np.load(os.path.join(ROOT, "tests", "golden", "mu0.npz"))
+    done = 0
+    for i in range(len(G["r_status"])):
+        if int(G["r_status"][i]) != 1 or done >= 6:
+            continue
+        k = int(G["r_gidx"][i])
+        kappa = G[f"kappa{k}"]
+        h = kappa.shape[0]
+        if h > 20:
+            continue
+        p = np.concatenate([[0], G["r_p"][i][:h - 1]]).astype(np.int64)[None]
+        Mb = np.eye(h, dtype=np.int64)
+        _, _, _, _, st_ref = ref.coni_zpk_batch(kappa, Mb, p, 100, 13, 20)
+        _, _, _, _, st = emu.coni_zpk_batch(kappa, Mb, p, 100, 13, 20)
+        if st_ref[0] in (0, 1):
+            assert st[0] == st_ref[0], i
+            done += 1
+    assert done >= 3
