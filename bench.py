@@ -461,6 +461,7 @@ def zpk_rates(device, threads):
     n_dirs = sum(len(g[2]) for g in data)
     out = {"workload": f"{len(data)} reference dataset geometries (h11 3..9), {n_dirs} p-vectors, the points and "
                        f"PFVs of dilation above D0"}
+    items = [dict(kappa=g[0], Mbasis=g[1], ps=g[2][:, 1:], Q=g[3], M0min=g[4]) for g in data]
     for D0 in (20, 150):
         for g in data[:2]:
             gpu.coni_zpk_points(g[0], g[1], g[2], g[3], g[4], D0, device=device)     # (warm)
@@ -468,7 +469,7 @@ def zpk_rates(device, threads):
         for _ in range(2):
             t0 = time.perf_counter()
             dev = pts = bad = 0
-            for g in data:
+            for g in data:                      # (one device call per geometry, as the reference's czk_batch)
                 M, Kn, q, pidx, st, secs = gpu.coni_zpk_points(g[0], g[1], g[2], g[3], g[4], D0, device=device)
                 dev += secs
                 pts += len(q)
@@ -477,10 +478,12 @@ def zpk_rates(device, threads):
             if best is None or wall < best[0]:
                 best = (wall, dev, pts, bad)
         t0 = time.perf_counter()
-        n_pfv = sum(len(zpk.coni_zpk(g[0], g[1], g[2][:, 1:], g[3], D0, M0min=g[4], device=device)[2]) for g in data)
+        n_pfv = sum(len(r[2]) for r in zpk.coni_zpk_multi(items, D0, device=device))
         pfv_wall = time.perf_counter() - t0
         ent = {"points": int(best[2]), "not_decided": int(best[3]), "device_kernel_s": best[1], "wall_s": best[0],
-               "directions_per_s": n_dirs / best[0], "pfvs": int(n_pfv), "pfvs_wall_s": pfv_wall}
+               "directions_per_s": n_dirs / best[0], "pfvs": int(n_pfv), "pfvs_wall_s": pfv_wall,
+               "what": "one device call per geometry (pfg_coni_zpk_batch); pfvs through "
+                       "pfvs_b200.zpk.coni_zpk_multi (the kernel, the device post-processing, the dilation filter)"}
         if ref.available():
             jobs = [(g, c) for g in data for c in np.array_split(g[2], max(1, min(4 * threads, len(g[2]) // 8)))]
             t1 = time.perf_counter()

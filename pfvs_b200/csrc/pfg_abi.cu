@@ -1048,52 +1048,66 @@ mu_fail:
 // ---------------------------------------------------------------------------
 namespace {
 
-constexpr long long ZPK_STEP_BUDGET = 100000000ll;  // search nodes + (j, M0) steps per direction
+constexpr long long ZPK_STEP_BUDGET = 100000000ll;  // search nodes + (j, M0) steps per lane and direction
 
 struct EventPair {
     cudaEvent_t a = nullptr, b = nullptr;
     ~EventPair() { if (a) cudaEventDestroy(a); if (b) cudaEventDestroy(b); }
 };
 
-// k_zpk over the n_p directions; the points of the directions with status 0
+// one call: one geometry (h, Q, M0min, kappa, Mbasis) and n_p directions
+// (rows of ps_stride entries)
+struct ZpkCall {
+    int h;
+    int64_t Q, M0min;
+    const int64_t *kappa, *Mbasis;
+    int64_t n_p;
+    const int64_t *ps;
+    int ps_stride;
+    int64_t D0, max_out;
+    int device;
+};
+
+// k_zpk over the call's directions; the points of the directions with status 0
 // into host rows (MH wide), the statuses into `status`.  kappa stays on the
-// device in W_MU_K (*dkappa).  Returns 0 or 1 with err set.
-int zpk_points(Workspace &W, int h, const int64_t *kappa, const int64_t *Mbasis, int64_t n_p, const int64_t *ps,
-               int64_t Q, int64_t M0min, int64_t D0, int64_t max_out, int device, int32_t *status,
-               std::vector<int64_t> &M, std::vector<int64_t> &Kn, std::vector<int64_t> &q, std::vector<int64_t> &pidx,
-               double &secs, int &nsm, int64_t **dkappa, char *err)
+// device (*dkappa).  Returns 0 or 1 with err set.
+int zpk_points(Workspace &W, const ZpkCall &C, int32_t *status, std::vector<int64_t> &M, std::vector<int64_t> &Kn,
+               std::vector<int64_t> &q, std::vector<int64_t> &pidx, double &secs, int &nsm, int64_t **dkappa,
+               char *err)
 {
     cudaError_t e;
 #define ZCK(x) do { e = (x); if (e != cudaSuccess) { snprintf(err, 256, "%s (%s:%d)", cudaGetErrorString(e), \
     __FILE__, __LINE__); return 1; } } while (0)
+    const int64_t ksz = (int64_t)C.h * C.h * C.h, msz = (int64_t)C.h * C.h;
     int bps = 0;
-    ZCK(cudaSetDevice(device));
-    ZCK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device));
+    ZCK(cudaSetDevice(C.device));
+    ZCK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, C.device));
     ZCK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_zpk, 128, 0));
-    const int grid = (int)std::min<int64_t>((n_p + 3) / 4, (int64_t)nsm * std::max(1, std::min(bps, 4)));
-    int64_t *dk, *dmb, *dps, *dM, *dK, *dq, *dp; int32_t *dst; ZpkScratch *dscr; unsigned *dctr;
-    ZCK(ws_get(W, W_MU_K, (size_t)h * h * h * 8, (void **)&dk));
-    ZCK(ws_get(W, W_ZK_MB, (size_t)h * h * 8, (void **)&dmb));
-    ZCK(ws_get(W, W_ZK_PS, (size_t)n_p * h * 8, (void **)&dps));
-    ZCK(ws_get(W, W_ZK_ST, (size_t)n_p * 4, (void **)&dst));
+    const int grid = (int)std::min<int64_t>((C.n_p + 3) / 4, (int64_t)nsm * std::max(1, std::min(bps, 4)));
+    int64_t *dk, *dmb, *dps, *dM, *dK, *dq, *dp; int32_t *dst;
+    ZpkScratch *dscr; unsigned *dctr;
+    ZCK(ws_get(W, W_MU_K, (size_t)ksz * 8, (void **)&dk));
+    ZCK(ws_get(W, W_ZK_MB, (size_t)msz * 8, (void **)&dmb));
+    ZCK(ws_get(W, W_ZK_PS, (size_t)C.n_p * C.ps_stride * 8, (void **)&dps));
+    ZCK(ws_get(W, W_ZK_ST, (size_t)C.n_p * 4, (void **)&dst));
     ZCK(ws_get(W, W_ZK_SCR, (size_t)grid * 4 * sizeof(ZpkScratch), (void **)&dscr));
     ZCK(ws_get(W, W_ZK_CTR, 64, (void **)&dctr));
-    ZCK(cudaMemcpy(dk, kappa, (size_t)h * h * h * 8, cudaMemcpyHostToDevice));
-    ZCK(cudaMemcpy(dmb, Mbasis, (size_t)h * h * 8, cudaMemcpyHostToDevice));
-    ZCK(cudaMemcpy(dps, ps, (size_t)n_p * h * 8, cudaMemcpyHostToDevice));
+    ZCK(cudaMemcpy(dk, C.kappa, (size_t)ksz * 8, cudaMemcpyHostToDevice));
+    ZCK(cudaMemcpy(dmb, C.Mbasis, (size_t)msz * 8, cudaMemcpyHostToDevice));
+    ZCK(cudaMemcpy(dps, C.ps, (size_t)C.n_p * C.ps_stride * 8, cudaMemcpyHostToDevice));
     *dkappa = dk;
     EventPair ev;
     ZCK(cudaEventCreate(&ev.a));
     ZCK(cudaEventCreate(&ev.b));
-    unsigned long long cap = std::max<unsigned long long>(1ull << 14, (unsigned long long)n_p * 8), count = 0;
+    unsigned long long cap = std::max<unsigned long long>(1ull << 14, (unsigned long long)C.n_p * 8), count = 0;
     for (int pass = 0; pass < 2; ++pass) {
         ZCK(ws_get(W, W_ZK_M, cap * MH * 8, (void **)&dM));
         ZCK(ws_get(W, W_ZK_K, cap * MH * 8, (void **)&dK));
         ZCK(ws_get(W, W_ZK_Q, cap * 8, (void **)&dq));
         ZCK(ws_get(W, W_ZK_P, cap * 8, (void **)&dp));
         ZCK(cudaMemset(dctr, 0, 64));
-        ZpkArgs A{h, dk, dmb, dps, (int)n_p, Q, M0min, D0, max_out, dctr, dscr, dst,
-                  (unsigned long long *)(dctr + 2), cap, dM, dK, dq, dp, ZPK_STEP_BUDGET};
+        ZpkArgs A{C.h, dk, dmb, dps, C.ps_stride, (int)C.n_p, C.Q, C.M0min, C.D0, C.max_out,
+                  dctr, dscr, dst, (unsigned long long *)(dctr + 2), cap, dM, dK, dq, dp, ZPK_STEP_BUDGET};
         ZCK(cudaEventRecord(ev.a));
         k_zpk<<<grid, 128>>>(A);
         ZCK(cudaGetLastError());
@@ -1105,7 +1119,7 @@ int zpk_points(Workspace &W, int h, const int64_t *kappa, const int64_t *Mbasis,
     float ms = 0.f;
     ZCK(cudaEventElapsedTime(&ms, ev.a, ev.b));
     secs = ms * 1e-3;
-    ZCK(cudaMemcpy(status, dst, (size_t)n_p * 4, cudaMemcpyDeviceToHost));
+    ZCK(cudaMemcpy(status, dst, (size_t)C.n_p * 4, cudaMemcpyDeviceToHost));
     std::vector<int64_t> aM(count * MH), aK(count * MH), aq(count), ap(count);
     if (count) {
         ZCK(cudaMemcpy(aM.data(), dM, count * MH * 8, cudaMemcpyDeviceToHost));
@@ -1123,6 +1137,61 @@ int zpk_points(Workspace &W, int h, const int64_t *kappa, const int64_t *Mbasis,
     }
     return 0;
 #undef ZCK
+}
+
+// the call's points -> PFVs on the device (the coniZpM post-processing stage)
+int zpk_pfvs(Workspace &W, const ZpkCall &C, int32_t *status, pfg_pfv_output *out)
+{
+    std::vector<int64_t> M, Kn, q, pidx;
+    int nsm = 148;
+    int64_t *dk = nullptr;
+    PfvSink sink;
+    if (zpk_points(W, C, status, M, Kn, q, pidx, out->seconds_gpu, nsm, &dk, out->err)) {
+        cudaGetLastError();
+        return 1;
+    }
+    const size_t n = q.size();
+    if (n) {
+        cudaError_t e;
+        int64_t *dM, *dK, *dq, *dp, launches = 0;
+        Dir *ddirs; Geo *dgeo;
+        std::vector<Dir> dirs(C.n_p);
+        for (int64_t i = 0; i < C.n_p; ++i) {
+            dirs[i] = Dir{};
+            dirs[i].geo = 0; dirs[i].h = C.h; dirs[i].d = C.h - 1;
+        }
+        Geo geo{};
+        geo.h = C.h; geo.d = C.h - 1; geo.coni = 1; geo.Q = C.Q; geo.linmin = C.M0min; geo.koff = 0;
+#define ZCK2(x) do { e = (x); if (e != cudaSuccess) { snprintf(out->err, sizeof out->err, "%s (%s:%d)", \
+    cudaGetErrorString(e), __FILE__, __LINE__); cudaGetLastError(); sink.release(); return 1; } } while (0)
+        ZCK2(ws_get(W, W_OM, n * MH * 8, (void **)&dM));
+        ZCK2(ws_get(W, W_OK, n * MH * 8, (void **)&dK));
+        ZCK2(ws_get(W, W_OQ, n * 8, (void **)&dq));
+        ZCK2(ws_get(W, W_OP, n * 8, (void **)&dp));
+        ZCK2(ws_get(W, W_DIRS, (size_t)C.n_p * sizeof(Dir), (void **)&ddirs));
+        ZCK2(ws_get(W, W_GEO, sizeof(Geo), (void **)&dgeo));
+        ZCK2(cudaMemcpy(dM, M.data(), n * MH * 8, cudaMemcpyHostToDevice));
+        ZCK2(cudaMemcpy(dK, Kn.data(), n * MH * 8, cudaMemcpyHostToDevice));
+        ZCK2(cudaMemcpy(dq, q.data(), n * 8, cudaMemcpyHostToDevice));
+        ZCK2(cudaMemcpy(dp, pidx.data(), n * 8, cudaMemcpyHostToDevice));
+        ZCK2(cudaMemcpy(ddirs, dirs.data(), (size_t)C.n_p * sizeof(Dir), cudaMemcpyHostToDevice));
+        ZCK2(cudaMemcpy(dgeo, &geo, sizeof(Geo), cudaMemcpyHostToDevice));
+#undef ZCK2
+        if (pfv_stage(W, nsm, ddirs, dgeo, dk, dM, dK, dq, dp, n, 0, std::max(3, C.h), &sink, launches, out->err)) {
+            cudaGetLastError();
+            sink.release();
+            return 1;
+        }
+    }
+    size_t np_ = 0;
+    for (auto &c : sink.chunks) np_ += c.n;
+    out->n = (int64_t)np_;
+    out->n_points = (int64_t)n;
+    if (sink.chunks.size() == 1) {
+        out->K = sink.chunks[0].K; out->M = sink.chunks[0].M; out->pidx = sink.chunks[0].pidx;
+        sink.chunks.clear();
+    }
+    return 0;
 }
 
 bool zpk_args_ok(int h, const int64_t *kappa, const int64_t *Mbasis, int64_t n_p, const int64_t *ps,
@@ -1146,11 +1215,11 @@ extern "C" int pfg_coni_zpk_batch(int h, const int64_t *kappa, const int64_t *Mb
     if (n_p == 0) return 0;
     Workspace &W = workspace(device);
     std::lock_guard<std::mutex> lock(W.mu);
+    const ZpkCall C{h, Q, M0min, kappa, Mbasis, n_p, ps, h, D0, max_out, device};
     std::vector<int64_t> M, Kn, q, pidx;
     int nsm = 148;
     int64_t *dk = nullptr;
-    if (zpk_points(W, h, kappa, Mbasis, n_p, ps, Q, M0min, D0, max_out, device, status, M, Kn, q, pidx,
-                   out->seconds_gpu, nsm, &dk, out->err)) {
+    if (zpk_points(W, C, status, M, Kn, q, pidx, out->seconds_gpu, nsm, &dk, out->err)) {
         cudaGetLastError();
         return 1;
     }
@@ -1184,56 +1253,6 @@ extern "C" int pfg_coni_zpk_pfvs(int h, const int64_t *kappa, const int64_t *Mba
     if (n_p == 0) return 0;
     Workspace &W = workspace(device);
     std::lock_guard<std::mutex> lock(W.mu);
-    std::vector<int64_t> M, Kn, q, pidx;
-    int nsm = 148;
-    int64_t *dk = nullptr;
-    PfvSink sink;
-    int rc = 0;
-    if (zpk_points(W, h, kappa, Mbasis, n_p, ps, Q, M0min, D0, max_out, device, status, M, Kn, q, pidx,
-                   out->seconds_gpu, nsm, &dk, out->err)) {
-        cudaGetLastError();
-        return 1;
-    }
-    const size_t n = q.size();
-    out->n_points = 0;
-    if (n) {
-        cudaError_t e;
-        int64_t *dM, *dK, *dq, *dp, launches = 0;
-        Dir *ddirs; Geo *dgeo;
-        std::vector<Dir> dirs(n_p);
-        for (auto &D : dirs) { D = Dir{}; D.geo = 0; D.h = h; D.d = h - 1; }
-        Geo g{};
-        g.h = h; g.d = h - 1; g.coni = 1; g.Q = Q; g.linmin = M0min; g.koff = 0;
-#define ZCK2(x) do { e = (x); if (e != cudaSuccess) { snprintf(out->err, sizeof out->err, "%s (%s:%d)", \
-    cudaGetErrorString(e), __FILE__, __LINE__); rc = 1; goto zfail; } } while (0)
-        ZCK2(ws_get(W, W_OM, n * MH * 8, (void **)&dM));
-        ZCK2(ws_get(W, W_OK, n * MH * 8, (void **)&dK));
-        ZCK2(ws_get(W, W_OQ, n * 8, (void **)&dq));
-        ZCK2(ws_get(W, W_OP, n * 8, (void **)&dp));
-        ZCK2(ws_get(W, W_DIRS, (size_t)n_p * sizeof(Dir), (void **)&ddirs));
-        ZCK2(ws_get(W, W_GEO, sizeof(Geo), (void **)&dgeo));
-        ZCK2(cudaMemcpy(dM, M.data(), n * MH * 8, cudaMemcpyHostToDevice));
-        ZCK2(cudaMemcpy(dK, Kn.data(), n * MH * 8, cudaMemcpyHostToDevice));
-        ZCK2(cudaMemcpy(dq, q.data(), n * 8, cudaMemcpyHostToDevice));
-        ZCK2(cudaMemcpy(dp, pidx.data(), n * 8, cudaMemcpyHostToDevice));
-        ZCK2(cudaMemcpy(ddirs, dirs.data(), (size_t)n_p * sizeof(Dir), cudaMemcpyHostToDevice));
-        ZCK2(cudaMemcpy(dgeo, &g, sizeof(Geo), cudaMemcpyHostToDevice));
-        if (pfv_stage(W, nsm, ddirs, dgeo, dk, dM, dK, dq, dp, n, 0, h, &sink, launches, out->err)) { rc = 1; goto zfail; }
-#undef ZCK2
-    }
-    {
-        size_t np_ = 0;
-        for (auto &c : sink.chunks) np_ += c.n;
-        out->n = (int64_t)np_;
-        out->n_points = (int64_t)n;
-        if (sink.chunks.size() == 1) {
-            out->K = sink.chunks[0].K; out->M = sink.chunks[0].M; out->pidx = sink.chunks[0].pidx;
-            sink.chunks.clear();
-        }
-    }
-    return 0;
-zfail:
-    cudaGetLastError();
-    sink.release();
-    return rc;
+    const ZpkCall C{h, Q, M0min, kappa, Mbasis, n_p, ps, h, D0, max_out, device};
+    return zpk_pfvs(W, C, status, out);
 }

@@ -35,8 +35,9 @@
 //      triangular (Gamma's basis in Lambda coordinates), kv spanning ker W;
 //      Hdet = det H, Hadj = Hdet H^-T, Cs / Cden solving W c1 = v for v in
 //      Gamma, HT = Hadj V^T, w = l Cs O^T V^T, lk = l . kv.
-//   5. Lane 0: every x != 0 with x^T Gr x D0 < Q L by a depth-first search
-//      with exact partial sums (Gr x, HT x, w . x, x^T Gr x) carried down the
+//   5. Every x != 0 with x^T Gr x D0 < Q L by depth-first walks, one per lane
+//      (the nodes two levels below the top dealt to the lanes in turn), with
+//      exact partial sums (Gr x, HT x, w . x, x^T Gr x) carried down the
 //      levels; per short x the (j, M0) ranges above and the points, emitted
 //      with M = Binter c, Kn = Z Binter c, q = c^T mat c = -M . Kn.
 //
@@ -88,11 +89,16 @@ struct ZpkScratch {
     int64_t HT[32 * 32];                      // Hadj V^T (n x n)
     int64_t wv[32];                           // l Cs O^T V^T
     double R[32 * 32];                        // FP64 Cholesky factor of Gr
-    i128 gx[31 * 32], hx[31 * 32];            // exact partial sums per level (search)
-    i128 wx[32], vals[32];
-    int64_t x[32], lo[32], hi[32];
-    double rem[32], aoff[32], ofs[32];
-    i128 c1[32];                              // c1 of the current short vector
+    // the search, one walk per lane: state interleaved by lane ([..][lane])
+    i128 gx[31 * 32 * 32], hx[31 * 32 * 32];  // exact partial sums per level: Gr x, HT x
+    i128 wx[32 * 32], vals[32 * 32];          // w . x, x^T Gr x per level
+    int64_t x[32 * 32], lo[32 * 32], hi[32 * 32];
+    double rem[32 * 32], aoff[32 * 32], ofs[32 * 32];
+    i128 c1[32 * 32];                         // c1 of the lane's current short vector
+    double rad, g2;                           // the search radius, the dot products' rounding factor
+    i128 QL;                                  // Q L
+    unsigned long long nout;                  // points of the direction so far
+    int abort;                                // a lane ended with an error: the others stop
     LllMem<32> L;                             // LLL working set
     int64_t Lb[31 * 32];                      // its rows
 };
@@ -101,7 +107,8 @@ struct ZpkArgs {
     int h;
     const int64_t *kappa;                     // h^3
     const int64_t *Mbasis;                    // h^2
-    const int64_t *ps;                        // (n_p, h), p[0] = 0
+    const int64_t *ps;                        // rows of ps_stride entries, p[0] = 0 in the first h
+    int ps_stride;
     int n_p;
     int64_t Q, M0min, D0, max_out;
     unsigned *next;                           // work counter
@@ -112,6 +119,21 @@ struct ZpkArgs {
     int64_t *M, *Kn, *q, *pidx;               // rows of MH (first h entries), (cap,)
     long long budget;                         // search nodes + (j, M0) steps per direction
 };
+
+// int128 quotient (truncated, as C) and remainder, on the 64-bit path when both
+// operands fit (the common case here; the 128-bit division is a long software routine)
+__device__ __forceinline__ i128 q128(i128 a, i128 b)
+{
+    return fits64(a) && fits64(b) ? (i128)((int64_t)a / (int64_t)b) : a / b;
+}
+__device__ __forceinline__ i128 r128(i128 a, i128 b)
+{
+    return fits64(a) && fits64(b) ? (i128)((int64_t)a % (int64_t)b) : a % b;
+}
+__device__ __forceinline__ i128 fdivq(i128 a, i128 b)
+{
+    return fits64(a) && fits64(b) ? (i128)fdiv64((int64_t)a, (int64_t)b) : fdiv128(a, b);
+}
 
 // a b + c into *r; true on overflow
 __device__ __forceinline__ bool muladd_ovf(i128 a, i128 b, i128 c, i128 *r)
@@ -257,7 +279,7 @@ struct ZpkDir { int64_t Hdet, Cden, L, sn, sd, lk; };
 __device__ int zpk_setup(const ZpkArgs &P, int k, ZpkScratch *W, ZpkDir &D, int lane)
 {
     const int h = P.h, m = h - 1, n = h - 2;
-    const int64_t *kap = P.kappa, *Mb = P.Mbasis, *p = P.ps + (int64_t)k * h;
+    const int64_t *kap = P.kappa, *Mb = P.Mbasis, *p = P.ps + (int64_t)k * P.ps_stride;
     bool bad = false;
     // 1. Z = kappa . p, T = Z p (into x), v = T^T Mbasis (into wv)
     for (int e = lane; e < h * h; e += 32) {
@@ -554,15 +576,15 @@ __device__ int zpk_setup(const ZpkArgs &P, int k, ZpkScratch *W, ZpkDir &D, int 
     return ZPK_OK;
 }
 
-// one point c = j c1 + t kv: M = Binter c, Kn = Z Binter c, q = -M . Kn (lane 0)
-__device__ int zpk_emit(const ZpkArgs &P, int k, ZpkScratch *W, i128 j, i128 t, long long &nout)
+// one point c = j c1 + t kv: M = Binter c, Kn = Z Binter c, q = -M . Kn (one lane)
+__device__ int zpk_emit(const ZpkArgs &P, int k, ZpkScratch *W, i128 j, i128 t, int lane)
 {
     const int h = P.h, m = h - 1;
-    if (nout >= P.max_out) return ZPK_MAX_OUT;
     int64_t c[32], Mr[32], Kr[32];
     for (int i = 0; i < m; ++i) {
         i128 s;
-        if (mul_ovf(j, W->c1[i], &s) || muladd_ovf(t, (i128)W->kv[i], s, &s) || !fits64(s)) return ZPK_OVF_POINT;
+        if (mul_ovf(j, W->c1[(i << 5) + lane], &s) || muladd_ovf(t, (i128)W->kv[i], s, &s) || !fits64(s))
+            return ZPK_OVF_POINT;
         c[i] = (int64_t)s;
     }
     i128 mk = 0;
@@ -579,8 +601,8 @@ __device__ int zpk_emit(const ZpkArgs &P, int k, ZpkScratch *W, i128 j, i128 t, 
         if (add_ovf(mk, (i128)Mr[i] * (i128)Kr[i], &mk)) return ZPK_OVF_POINT;
     }
     if (!fits64(-mk)) return ZPK_OVF_POINT;
+    if (atomicAdd(&W->nout, 1ull) >= (unsigned long long)P.max_out) return ZPK_MAX_OUT;
     const unsigned long long slot = atomicAdd(P.count, 1ull);
-    ++nout;
     if (slot < P.cap) {
         for (int i = 0; i < MH; ++i) {
             P.M[slot * MH + i] = i < h ? Mr[i] : 0;
@@ -592,40 +614,59 @@ __device__ int zpk_emit(const ZpkArgs &P, int k, ZpkScratch *W, i128 j, i128 t, 
     return ZPK_OK;
 }
 
-// the points of the short vector x (level-0 sums hx = HT x, wx = w . x; val = x^T Gr x)
-__device__ int zpk_per_short(const ZpkArgs &P, int k, ZpkScratch *W, const ZpkDir &D, i128 QL, i128 val,
-                             long long &nout, long long &steps)
+// the points of the lane's short vector x (level-0 sums hx = HT x, wx = w . x; val = x^T Gr x)
+__device__ int zpk_per_short(const ZpkArgs &P, int k, ZpkScratch *W, const ZpkDir &D, i128 val, long long &steps,
+                             int lane)
 {
     const int n = P.h - 2, m = P.h - 1;
+    const int64_t *x = W->x;
     uint64_t gu = 0;
-    for (int i = 0; i < n; ++i) gu = gcd64(gu, uabs64(W->x[i]));
-    const i128 g = (i128)gu, kn = val / (g * g);                       // kn = L K'^T S K'
+    for (int i = 0; i < n; ++i) gu = gcd64(gu, uabs64(x[(i << 5) + lane]));
+    const i128 g = (i128)gu, kn = gu == 1 ? val : q128(val, g * g);     // kn = L K'^T S K'
     // o = Hdet / gcd(Hdet, Hadj y'): the order of K' = K / g in Lambda / Gamma
     uint64_t og = (uint64_t)D.Hdet;
     for (int i = 0; i < n && og != 1; ++i) {
-        const uint64_t r = (uint64_t)(uabs(W->hx[i] / g) % (u128)og);
+        const i128 hv = W->hx[(i << 5) + lane];
+        const u128 av = uabs(gu == 1 ? hv : q128(hv, g));
+        const uint64_t r = (av >> 64) ? (uint64_t)(av % (u128)og) : (uint64_t)av % og;
         if (r) og = gcd64(og, r);
     }
     const i128 o = (i128)((uint64_t)D.Hdet / og);
     // l . c1 = o (w . y') / Cden for W c1 = o K'
     i128 num, den;
-    if (mul_ovf(o, W->wx[0], &num) || mul_ovf(g, (i128)D.Cden, &den)) return ZPK_OVF_K;
-    if (num % den) return ZPK_INEXACT_K;
-    const i128 lc1 = num / den, lk = D.lk, alk = lk < 0 ? -lk : lk;
+    if (mul_ovf(o, W->wx[lane], &num) || mul_ovf(g, (i128)D.Cden, &den)) return ZPK_OVF_K;
+    if (r128(num, den)) return ZPK_INEXACT_K;
+    const i128 QL = W->QL, lc1 = q128(num, den), lk = D.lk, alk = lk < 0 ? -lk : lk;
     // j: j o > g D0 and g j o kn < Q L
     i128 gLsn, gokn, gD0;
     if (mul_ovf(g, (i128)D.L, &gLsn) || mul_ovf(gLsn, (i128)D.sn, &gLsn) || mul_ovf(g, o, &gokn) ||
         mul_ovf(gokn, kn, &gokn) || mul_ovf(g, (i128)P.D0, &gD0)) return ZPK_OVF_K;
-    const i128 jlo = fdiv128(gD0, o) + 1, jhi = (QL - 1) / gokn;
+    i128 jlo = fdivq(gD0, o) + 1, jhi = q128(QL - 1, gokn);
     if (jlo > jhi) return ZPK_OK;
     // per j: M0 = j lc1 + t lk >= M0min in one residue class mod |lk|, with
     // g L sn M0^2 < sd j o (Q L - g j o kn); a float screen (relative margin 1e-9)
     // skips the j whose smallest M0 fails, the rest is exact
-    const i128 step = ((lc1 % alk) + alk) % alk, m0m = (((i128)P.M0min % alk) + alk) % alk;
-    i128 res;
-    if (mul_ovf(jlo % alk, step, &res)) return ZPK_OVF_K;
-    res %= alk;
     const double gLsn_d = (double)gLsn, sdo_d = (double)D.sd * (double)o;
+    {
+        // the screen fails at every j where even M0 = M0min does: outside the roots of
+        // sd o j (Q L - g o kn j) = T, T = (M0min^2 g L sn - 1) / (1 + 1e-9) (a concave
+        // parabola in j), so the loop runs between the roots, widened by a relative 1e-6
+        // and two steps on each side (far beyond the roots' rounding)
+        const double T = ((double)P.M0min * (double)P.M0min * gLsn_d - 1.0) / (1.0 + 1e-9);
+        const double B = (double)QL, C = (double)gokn, Ta = T / sdo_d;
+        const double disc = B * B - 4.0 * C * Ta;
+        if (disc < -1e-6 * B * B) return ZPK_OK;                   // no j reaches T
+        const double sq = sqrt(fmax(disc, 0.0));
+        const double r1 = Ta > 0 ? 2.0 * Ta / (B + sq) : 0.0, r2 = (B + sq) / (2.0 * C);
+        const double jl = floor(r1 - 1e-6 * (r1 + 1.0)) - 2.0, jr = ceil(r2 + 1e-6 * (r2 + 1.0)) + 2.0;
+        if (jl > (double)jlo && jl < 1e30) jlo = (i128)jl;
+        if (jr < (double)jhi && jr > -1e30) jhi = (i128)jr;
+        if (jlo > jhi) return ZPK_OK;
+    }
+    const i128 step = r128(r128(lc1, alk) + alk, alk), m0m = r128(r128((i128)P.M0min, alk) + alk, alk);
+    i128 res;
+    if (mul_ovf(r128(jlo, alk), step, &res)) return ZPK_OVF_K;
+    res = r128(res, alk);
     bool have_c1 = false;
     for (i128 j = jlo; j <= jhi; ++j, res = res + step >= alk ? res + step - alk : res + step) {
         if (++steps > P.budget) return ZPK_BUDGET;
@@ -644,15 +685,17 @@ __device__ int zpk_per_short(const ZpkArgs &P, int k, ZpkScratch *W, const ZpkDi
             if (mul_ovf(M0, M0, &lhs) || mul_ovf(lhs, gLsn, &lhs)) break;      // (beyond R)
             if (lhs >= R) break;
             if (mul_ovf(j, lc1, &t1) || sub_ovf(M0, t1, &t1)) return ZPK_OVF_K;
-            if (t1 % lk) return ZPK_INEXACT_K;
+            if (r128(t1, lk)) return ZPK_INEXACT_K;
             if (!have_c1) {
                 // y = x V / g (Lambda coordinates of K'), v = o O^T y = o K', c1 = Cs v / Cden
                 i128 y[32], v[32];
                 for (int b = 0; b < n; ++b) {
                     i128 s = 0;
-                    for (int a = 0; a < n; ++a)
-                        if (W->x[a] && muladd_ovf((i128)W->x[a], (i128)W->L.B[a * 32 + b], s, &s)) return ZPK_OVF_K;
-                    y[b] = s / g;
+                    for (int a = 0; a < n; ++a) {
+                        const int64_t xa = x[(a << 5) + lane];
+                        if (xa && muladd_ovf((i128)xa, (i128)W->L.B[a * 32 + b], s, &s)) return ZPK_OVF_K;
+                    }
+                    y[b] = gu == 1 ? s : q128(s, g);
                 }
                 for (int i = 0; i < m; ++i) {
                     i128 s = 0;
@@ -665,24 +708,22 @@ __device__ int zpk_per_short(const ZpkArgs &P, int k, ZpkScratch *W, const ZpkDi
                     for (int kk = 0; kk < m; ++kk)
                         if (v[kk] && muladd_ovf((i128)W->Cs[i * 32 + kk], v[kk], s, &s)) return ZPK_OVF_K;
                     if (s % (i128)D.Cden) return ZPK_INEXACT_K;
-                    W->c1[i] = s / (i128)D.Cden;
+                    W->c1[(i << 5) + lane] = s / (i128)D.Cden;
                 }
                 have_c1 = true;
             }
-            const int rc = zpk_emit(P, k, W, j, t1 / lk, nout);
+            const int rc = zpk_emit(P, k, W, j, q128(t1, lk), lane);
             if (rc) return rc;
         }
     }
     return ZPK_OK;
 }
 
-// Step 5 (lane 0): every x != 0 with x^T Gr x D0 < Q L.  Pruning as the
-// dilation bound's search (pfg_mu0.cuh): the FP64 Cholesky R of Gr with
-// R^T R = Gr + E, |E| <= g1 |R^T||R|, so x^T Gr x >= |R x|^2 (1 - g1 C),
-// C = 2 ||R||_F^2 ||R^-1||_F^2, and a level's term is computed within g2 a_i;
-// leaves are decided exactly from the partial sums carried down the levels
-// (|x_i| < 2^20 keeps them far inside int128).
-__device__ int zpk_search(const ZpkArgs &P, int k, ZpkScratch *W, const ZpkDir &D)
+// lane 0, before the walks: the arguments, Q L, the FP64 Cholesky factor R of Gr
+// and the radius.  As the dilation bound's search (pfg_mu0.cuh): R^T R = Gr + E,
+// |E| <= g1 |R^T||R|, so x^T Gr x >= |R x|^2 (1 - g1 C), C = 2 ||R||_F^2 ||R^-1||_F^2,
+// and x^T Gr x D0 < Q L needs |R x|^2 < rad = Q L / D0 / (1 - g1 C).
+__device__ int zpk_prepare(const ZpkArgs &P, ZpkScratch *W, const ZpkDir &D)
 {
     const int n = P.h - 2;
     if (P.D0 < 1 || P.M0min < 1) return ZPK_ARGS;
@@ -712,74 +753,117 @@ __device__ int zpk_search(const ZpkArgs &P, int k, ZpkScratch *W, const ZpkDir &
         }
     }
     const double u = 0x1p-53;
-    const double g1 = (n + 1) * u / (1 - (n + 1) * u), g2 = n * u / (1 - n * u);
+    const double g1 = (n + 1) * u / (1 - (n + 1) * u);
     const double C = 2.0 * fR * fRi;
     if (!(g1 * C < 1e-6)) return ZPK_ILLCOND;
-    const double rad = (double)QL / (double)P.D0 / (1.0 - g1 * C) * (1.0 + 1e-12);
+    W->rad = (double)QL / (double)P.D0 / (1.0 - g1 * C) * (1.0 + 1e-12);
+    W->g2 = n * u / (1 - n * u);
+    W->QL = QL;
+    W->nout = 0;
+    W->abort = 0;
+    return ZPK_OK;
+}
+
+constexpr int ZPK_STOPPED = -1000;            // (internal) another lane of the warp failed
+
+// Step 5, one depth-first walk per lane over every x != 0 with x^T Gr x D0 < Q L:
+// the nodes that survive the pruning at the split level (two levels below the
+// top) are dealt to the lanes in turn, each lane walking the levels above in
+// full and below only under its own nodes.  A level's term is computed within
+// g2 a_i; leaves are decided exactly from the partial sums carried down the
+// levels (|x_i| < 2^20 keeps them far inside int128).
+__device__ int zpk_walk(const ZpkArgs &P, int k, ZpkScratch *W, const ZpkDir &D, int lane)
+{
+    const int n = P.h - 2, split = n > 2 ? n - 2 : 0;
+    const double *R = W->R, rad = W->rad, g2 = W->g2, u = 0x1p-53;
     i128 *gx = W->gx, *hx = W->hx, *wx = W->wx, *vals = W->vals;
     int64_t *x = W->x, *lo = W->lo, *hi = W->hi;
     double *rem = W->rem, *aoff = W->aoff, *ofs = W->ofs;
-    for (int kk = 0; kk < n; ++kk) { gx[n * 32 + kk] = 0; hx[n * 32 + kk] = 0; x[kk] = 0; }
-    wx[n] = 0; vals[n] = 0; rem[n] = rad;
+#define ZL(i) (((i) << 5) + lane)                 // entry i of this lane's vectors
+#define ZLL(l, kk) (((((l) << 5) + (kk)) << 5) + lane)   // entry kk of level l
+    for (int kk = 0; kk < n; ++kk) { gx[ZLL(n, kk)] = 0; hx[ZLL(n, kk)] = 0; x[ZL(kk)] = 0; }
+    wx[ZL(n)] = 0; vals[ZL(n)] = 0; rem[ZL(n)] = rad;
     auto enter = [&](int ii) -> bool {
         double o = 0, a = 0;
-        for (int j = ii + 1; j < n; ++j) { const double t = R[ii * 32 + j] * (double)x[j]; o += t; a += fabs(t); }
+        for (int j = ii + 1; j < n; ++j) { const double t = R[ii * 32 + j] * (double)x[ZL(j)]; o += t; a += fabs(t); }
         const double rii = R[ii * 32 + ii];
-        const double ctr = -o / rii, wd = sqrt(fmax(rem[ii + 1], 0.0)) / rii;
+        const double ctr = -o / rii, wd = sqrt(fmax(rem[ZL(ii + 1)], 0.0)) / rii;
         // rounding of the centre and width, as a multiple of a coordinate step: must stay below 1/2
         const double e = g2 * (fabs(ctr) + wd + 1.0 + a / rii) * 4.0 + 4.0 * u * (fabs(ctr) + wd);
         if (!(e < 0.5) || !(fabs(ctr) + wd < 1e6)) return false;
-        lo[ii] = (int64_t)floor(ctr - wd) - 1;
-        hi[ii] = (int64_t)ceil(ctr + wd) + 1;
-        aoff[ii] = a;
-        ofs[ii] = o;
-        x[ii] = lo[ii];
+        lo[ZL(ii)] = (int64_t)floor(ctr - wd) - 1;
+        hi[ZL(ii)] = (int64_t)ceil(ctr + wd) + 1;
+        aoff[ZL(ii)] = a;
+        ofs[ZL(ii)] = o;
+        x[ZL(ii)] = lo[ZL(ii)];
         return true;
     };
-    long long steps = 0, nout = 0;
+    long long steps = 0, dealt = 0;
     int i = n - 1;
     if (!enter(i)) return ZPK_ENTER;
     for (;;) {
         if (++steps > P.budget) return ZPK_BUDGET;
-        if (x[i] > hi[i]) {                                          // level done
+        if ((steps & 255) == 0 && *(volatile int *)&W->abort) return ZPK_STOPPED;
+        if (x[ZL(i)] > hi[ZL(i)]) {                                  // level done
             if (++i == n) break;
-            x[i]++;
+            x[ZL(i)]++;
             continue;
         }
-        const double t = R[i * 32 + i] * (double)x[i] + ofs[i];
-        const double a = fabs(R[i * 32 + i] * (double)x[i]) + aoff[i];
+        const double xi_d = (double)x[ZL(i)];
+        const double t = R[i * 32 + i] * xi_d + ofs[ZL(i)];
+        const double a = fabs(R[i * 32 + i] * xi_d) + aoff[ZL(i)];
         const double lb = fmax(fabs(t) - g2 * a, 0.0) * (1.0 - 4.0 * u);
-        const double r = rem[i + 1] - lb * lb * (1.0 - 4.0 * u);
-        if (r < 0) { x[i]++; continue; }                             // (rigorously) too long
-        const i128 xi = x[i];
+        const double r = rem[ZL(i + 1)] - lb * lb * (1.0 - 4.0 * u);
+        if (r < 0) { x[ZL(i)]++; continue; }                         // (rigorously) too long
+        if (i == split && ((dealt++) & 31) != lane) { x[ZL(i)]++; continue; }   // another lane's node
+        const i128 xi = x[ZL(i)];
         if (xi >= (1 << 20) || xi <= -(1 << 20)) return ZPK_COORD;
         for (int kk = 0; kk < n; ++kk) {
-            gx[i * 32 + kk] = gx[(i + 1) * 32 + kk] + (i128)W->Gr[kk * 32 + i] * xi;
-            hx[i * 32 + kk] = hx[(i + 1) * 32 + kk] + (i128)W->HT[kk * 32 + i] * xi;
+            gx[ZLL(i, kk)] = gx[ZLL(i + 1, kk)] + (i128)W->Gr[kk * 32 + i] * xi;
+            hx[ZLL(i, kk)] = hx[ZLL(i + 1, kk)] + (i128)W->HT[kk * 32 + i] * xi;
         }
-        wx[i] = wx[i + 1] + (i128)W->wv[i] * xi;
-        vals[i] = vals[i + 1] + xi * (2 * gx[(i + 1) * 32 + i] + (i128)W->Gr[i * 32 + i] * xi);
+        wx[ZL(i)] = wx[ZL(i + 1)] + (i128)W->wv[i] * xi;
+        vals[ZL(i)] = vals[ZL(i + 1)] + xi * (2 * gx[ZLL(i + 1, i)] + (i128)W->Gr[i * 32 + i] * xi);
         if (i > 0) {
-            rem[i] = r;
+            rem[ZL(i)] = r;
             --i;
             if (!enter(i)) return ZPK_ENTER;
             continue;
         }
-        if (vals[0] > 0) {                                           // a leaf, decided exactly
+        const i128 val = vals[ZL(0)];
+        if (val > 0) {                                               // a leaf, decided exactly
             i128 lhs;
-            if (mul_ovf(vals[0], (i128)P.D0, &lhs)) return ZPK_OVF_QL;
-            if (lhs < QL) {
-                const int rc = zpk_per_short(P, k, W, D, QL, vals[0], nout, steps);
+            if (mul_ovf(val, (i128)P.D0, &lhs)) return ZPK_OVF_QL;
+            if (lhs < W->QL) {
+                const int rc = zpk_per_short(P, k, W, D, val, steps, lane);
                 if (rc) return rc;
             }
         } else {
             bool nz = false;
-            for (int j = 0; j < n; ++j) nz |= x[j] != 0;
+            for (int j = 0; j < n; ++j) nz |= x[ZL(j)] != 0;
             if (nz) return ZPK_NONE;                                 // not positive definite (exactly)
         }
-        x[i]++;
+        x[ZL(i)]++;
     }
     return ZPK_OK;
+#undef ZL
+#undef ZLL
+}
+
+// Step 5 for the warp: the walks, then the status of the lowest lane that
+// failed (the others stop at their next poll).
+__device__ int zpk_search(const ZpkArgs &P, int k, ZpkScratch *W, const ZpkDir &D, int lane)
+{
+    int st = 0;
+    if (lane == 0) st = zpk_prepare(P, W, D);
+    st = __shfl_sync(FULL, st, 0);
+    __syncwarp();
+    if (st) return st;
+    int my = zpk_walk(P, k, W, D, lane);
+    if (my != ZPK_OK && my != ZPK_STOPPED) atomicExch(&W->abort, 1);
+    const unsigned bad = __ballot_sync(FULL, my != ZPK_OK && my != ZPK_STOPPED);
+    if (!bad) return ZPK_OK;
+    return __shfl_sync(FULL, my, __ffs((int)bad) - 1);
 }
 
 // One warp per direction, taken from a work counter.
@@ -796,10 +880,10 @@ __global__ void __launch_bounds__(128) k_zpk(ZpkArgs P)
         if (t >= (unsigned)P.n_p) break;
         ZpkDir D{};
         int st = P.h < 3 || P.h > ZPK_MAXH ? (int)ZPK_RANGE : zpk_setup(P, (int)t, W, D, lane);
-        if (st == ZPK_OK && lane == 0) st = zpk_search(P, (int)t, W, D);
-        st = __shfl_sync(FULL, st, 0);
+        if (st == ZPK_OK) st = zpk_search(P, (int)t, W, D, lane);
         if (lane == 0) P.status[t] = st;
         __syncwarp();
     }
 }
+
 }  // namespace pfg

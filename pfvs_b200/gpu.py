@@ -510,3 +510,4 @@ def coni_zpk_pfvs(kappa, Mbasis, ps, Q, M0min, D0, max_out=10**9, device=0):
     res = (K[:, :h].copy(), M[:, :h].copy(), pidx.copy(), st[:n], int(out.n_points), out.seconds_gpu)
     del owner
     return res
+

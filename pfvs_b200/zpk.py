@@ -57,49 +57,73 @@ def coni_zpk(kappa, Mbasis, ps, Q, D0, M0min=13, device=0, max_N_pfvs=1_000_000_
     status (the kernel's per p-vector), fallback (the rows searched by ZpM
     to their bound instead), n_points, seconds_gpu.
     """
+    item = dict(kappa=kappa, Mbasis=Mbasis, ps=ps, Q=Q, M0min=M0min)
+    return coni_zpk_multi([item], D0, device=device, max_N_pfvs=max_N_pfvs, return_info=return_info)[0]
+
+
+def coni_zpk_multi(items, D0, device=0, max_N_pfvs=1_000_000_000, return_info=False):
+    """
+    coni_zpk over several geometries (one device call per geometry, as the
+    reference's coniZpK is per geometry): items is a list of dicts with
+    kappa, Mbasis, ps, Q and optionally M0min (13).  Returns, per item, what
+    coni_zpk returns for it.
+    """
     if int(D0) != D0 or D0 < 1:
         raise ValueError(f"D0 must be a positive integer, got {D0}")
     D0 = int(D0)
-    kappa = np.asarray(kappa, dtype=np.int64)
-    h = kappa.shape[0]
-    ps = np.atleast_2d(np.asarray(ps, dtype=np.int64))
-    if len(ps) == 0:
-        raise ValueError("ps must be non-empty.")
-    if ps.shape[1] != h - 1:
-        raise ValueError(f"ps must have h11 - 1 = {h - 1} columns (no coni entry), got {ps.shape[1]}")
-    p_full = np.hstack([np.zeros((len(ps), 1), dtype=np.int64), ps])
-    K, M, pidx, st, n_points, secs = gpu.coni_zpk_pfvs(kappa, Mbasis, p_full, Q, M0min, D0,
-                                                       max_out=max_N_pfvs, device=device)
-    pieces = [(K, M, pidx)]
-    bad = np.flatnonzero(st != 0)
-    if len(bad):
-        bceil, bst = dilation.coni_dilation_bound_ceils(ps[bad], kappa, Q, device=device, return_status=True)
-        for i, b, s in zip(bad, bceil, bst):
-            if b <= 0:
-                why = ("s >= 0, or S not positive definite on the lattice orthogonal to p" if s == 1 else
-                       f"its dilation bound is not decided on the device (status {int(s)})")
-                raise IncompleteSearchError(f"p={ps[i].tolist()}: its PFVs above D0 cannot be enumerated ({why})")
-        Ds = np.maximum(bceil, D0)
-        dil = sorted(set(int(D) for D in Ds))
-        gid = {D: g for g, D in enumerate(dil)}
-        geoms = [dict(kappa=kappa, Mbasis=Mbasis, Q=Q, dilation=float(D), M0min=M0min) for D in dil]
-        K1, M1, pidx1, pst, _, _ = gpu.coni_pfvs_multi(geoms, p_full[bad],
-                                                       np.array([gid[int(D)] for D in Ds], dtype=np.int32),
-                                                       device=device)
-        if np.any(pst != 0):
-            j = int(np.flatnonzero(pst != 0)[0])
-            raise IncompleteSearchError(f"p={ps[bad[j]].tolist()}: coniZpM up to its dilation bound did not "
-                                        f"finish on the device (status {int(pst[j])})")
-        pieces.append((np.asarray(K1)[:, :h], np.asarray(M1)[:, :h], bad[np.asarray(pidx1, dtype=np.int64)]))
-    Ks = np.vstack([pc[0] for pc in pieces]).astype(np.int64)
-    Ms = np.vstack([pc[1] for pc in pieces]).astype(np.int64)
-    keys = np.concatenate([np.asarray(pc[2], dtype=np.int64) for pc in pieces])
-    num, den = dilations(kappa, p_full, Ks, Ms, keys)
-    above = np.array([int(a) > D0 * int(b) for a, b in zip(num, den)], dtype=bool)
-    Ks, Ms, keys = coni._canonical(Ks[above], Ms[above], keys[above])
-    if return_info:
-        return Ks, Ms, keys, dict(status=st, fallback=bad, n_points=n_points, seconds_gpu=secs)
-    return Ks, Ms, keys
+    out = []
+    for it in items:
+        kappa = np.asarray(it["kappa"], dtype=np.int64)
+        h = kappa.shape[0]
+        ps = np.atleast_2d(np.asarray(it["ps"], dtype=np.int64))
+        if len(ps) == 0:
+            raise ValueError("ps must be non-empty.")
+        if ps.shape[1] != h - 1:
+            raise ValueError(f"ps must have h11 - 1 = {h - 1} columns (no coni entry), got {ps.shape[1]}")
+        p_full = np.hstack([np.zeros((len(ps), 1), dtype=np.int64), ps])
+        g = dict(kappa=kappa, Mbasis=np.asarray(it["Mbasis"], dtype=np.int64), h=h, ps=ps, p_full=p_full,
+                 Q=int(it["Q"]), M0min=it.get("M0min", 13))
+        K, M, pidx, st, n_points, secs = gpu.coni_zpk_pfvs(kappa, g["Mbasis"], p_full, g["Q"], g["M0min"], D0,
+                                                           max_out=max_N_pfvs, device=device)
+        pieces = [(K, M, np.asarray(pidx, dtype=np.int64))]
+        bad = np.flatnonzero(st != 0)
+        if len(bad):
+            pieces.append(_fallback(g, bad, D0, device))
+        Ks = np.vstack([pc[0] for pc in pieces]).astype(np.int64)
+        Ms = np.vstack([pc[1] for pc in pieces]).astype(np.int64)
+        keys = np.concatenate([np.asarray(pc[2], dtype=np.int64) for pc in pieces])
+        num, den = dilations(kappa, p_full, Ks, Ms, keys)
+        above = np.array([int(a) > D0 * int(b) for a, b in zip(num, den)], dtype=bool)
+        Ks, Ms, keys = coni._canonical(Ks[above], Ms[above], keys[above])
+        if return_info:
+            out.append((Ks, Ms, keys, dict(status=st, fallback=bad, n_points=n_points, seconds_gpu=secs)))
+        else:
+            out.append((Ks, Ms, keys))
+    return out
+
+
+def _fallback(g, bad, D0, device):
+    """coniZpM up to max(the dilation bound, D0) on the device for the rows
+    `bad` of one geometry (pfvs/coni.py:614-625): (Ks, Ms, keys)."""
+    kappa, h = g["kappa"], g["h"]
+    bceil, bst = dilation.coni_dilation_bound_ceils(g["ps"][bad], kappa, g["Q"], device=device, return_status=True)
+    for i, b, s in zip(bad, bceil, bst):
+        if b <= 0:
+            why = ("s >= 0, or S not positive definite on the lattice orthogonal to p" if s == 1 else
+                   f"its dilation bound is not decided on the device (status {int(s)})")
+            raise IncompleteSearchError(f"p={g['ps'][i].tolist()}: its PFVs above D0 cannot be enumerated ({why})")
+    Ds = np.maximum(bceil, D0)
+    dil = sorted(set(int(D) for D in Ds))
+    gid = {D: j for j, D in enumerate(dil)}
+    geoms = [dict(kappa=kappa, Mbasis=g["Mbasis"], Q=g["Q"], dilation=float(D), M0min=g["M0min"]) for D in dil]
+    K1, M1, pidx1, pst, _, _ = gpu.coni_pfvs_multi(geoms, g["p_full"][bad],
+                                                   np.array([gid[int(D)] for D in Ds], dtype=np.int32),
+                                                   device=device)
+    if np.any(pst != 0):
+        j = int(np.flatnonzero(pst != 0)[0])
+        raise IncompleteSearchError(f"p={g['ps'][bad[j]].tolist()}: coniZpM up to its dilation bound did not "
+                                    f"finish on the device (status {int(pst[j])})")
+    return np.asarray(K1)[:, :h], np.asarray(M1)[:, :h], bad[np.asarray(pidx1, dtype=np.int64)]
 
 
 def coniZpK(data, ps, D0, Q=None, M0min=13, n_jobs=-1, max_N_pfvs=1_000_000_000, return_formal_pfvs=False,

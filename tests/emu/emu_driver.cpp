@@ -242,10 +242,12 @@ extern "C" long long emu_coni_zpk_batch(int h, const int64_t *kappa, const int64
                                         int64_t *q, int64_t *pidx, int32_t *status)
 {
     std::vector<ZpkScratch> scr(1);
+    memset((void *)scr.data(), 0xA5, sizeof(ZpkScratch));        // (the device's scratch is not zeroed either)
     unsigned next = 0;
     unsigned long long count = 0;
-    ZpkArgs A{h, kappa, Mbasis, ps, (int)n_p, Q, M0min, D0, max_out, &next, scr.data(), status, &count, cap,
+    ZpkArgs A{h, kappa, Mbasis, ps, h, (int)n_p, Q, M0min, D0, max_out, &next, scr.data(), status, &count, cap,
               M, Kn, q, pidx, budget};
     emu_run_warp(0, 0, 32, 1, [&] { k_zpk(A); });
     return (long long)count;
 }
+

@@ -67,7 +67,8 @@ def test_gpu_zpk_pfvs_equal_the_reference(D0):
     total = 0
     for g in range(N_GEO):
         kappa, Mb, ps, h, Q, M0min = _geo(g)
-        Ks, Ms, keys = zpk.coni_zpk(kappa, Mb, ps[:, 1:], Q, D0, M0min=M0min)
+        Ks, Ms, keys, info = zpk.coni_zpk(kappa, Mb, ps[:, 1:], Q, D0, M0min=M0min, return_info=True)
+        assert np.all(info["status"] == 0) and len(info["fallback"]) == 0, g
         got = np.hstack([keys[:, None], Ms, Ks]) if len(keys) else np.zeros((0, 1 + 2 * h), np.int64)
         want = Z[f"g{g}_d{D0}_pfvs"]
         np.testing.assert_array_equal(got, want, err_msg=f"geometry {g}")
@@ -103,3 +104,20 @@ def test_gpu_zpk_fallback_to_zpm_at_the_bound():
     assert len(info["fallback"]) == int(np.sum(per > 3)) > 0
     got = np.hstack([keys[:, None], Ms, Ks])
     np.testing.assert_array_equal(got, Z["g13_d20_pfvs"])
+
+
+def test_gpu_zpk_multi_equals_the_reference():
+    """coni_zpk_multi over the 30 geometries returns, per geometry, the
+    reference's coniZpK PFVs, and every direction is decided by the kernel."""
+    _need_gpu()
+    D0 = 20
+    items, hs = [], []
+    for g in range(N_GEO):
+        kappa, Mb, ps, h, Q, M0min = _geo(g)
+        items.append(dict(kappa=kappa, Mbasis=Mb, ps=ps[:, 1:], Q=Q, M0min=M0min))
+        hs.append(h)
+    res = zpk.coni_zpk_multi(items, D0, return_info=True)
+    for g, (Ks, Ms, keys, info) in enumerate(res):
+        assert np.all(info["status"] == 0), g
+        got = np.hstack([keys[:, None], Ms, Ks]) if len(keys) else np.zeros((0, 1 + 2 * hs[g]), np.int64)
+        np.testing.assert_array_equal(got, Z[f"g{g}_d{D0}_pfvs"], err_msg=f"geometry {g}")

@@ -101,3 +101,54 @@ def test_device_zpk_no_bound_directions_match_the_reference():
             assert st[0] == st_ref[0], i
             done += 1
     assert done >= 3
+
+
+def test_zpk_driver_host_logic(monkeypatch):
+    """pfvs_b200.zpk.coni_zpk_multi with the emulated kernel and the oracle's
+    post-processing standing in for the device: each geometry's PFVs are the
+    reference's coniZpK PFVs (tests/golden/zpk.npz: dilation > D0, once each,
+    sorted by p-vector then (M, K)), and a direction the kernel drops (more
+    points than max_N_pfvs) goes to coniZpM up to max(its bound, D0)."""
+    from oracle import postproc
+    from pfvs_b200 import dilation, gpu, zpk
+    D0 = 20
+    gs = [5, 13, 15, 17]
+
+    def fake_pfvs(kappa, Mbasis, ps, Q, M0min, D0_, max_out=10**9, device=0):
+        h = ps.shape[1]
+        M, Kn, q, pidx, st = emu.coni_zpk_batch(kappa, Mbasis, ps, Q, M0min, D0_, max_out=max_out)
+        ok = st[pidx] == 0
+        K1, M1, k1 = postproc.pfvs_from_points(M[ok], Kn[ok], q[ok], pidx[ok], kappa, h, Q, M0min)
+        return (np.asarray(K1, np.int64).reshape(-1, h), np.asarray(M1, np.int64).reshape(-1, h),
+                np.asarray(k1, np.int64), st, int(ok.sum()), 0.0)
+
+    searched = []
+
+    def fake_bounds(ps, kappa, Q, device=0, return_status=False):
+        return np.full(len(ps), 400, np.int64), np.zeros(len(ps), np.int32)
+
+    def fake_zpm(geoms, ps, pgeo, device=0):
+        searched.append([g["dilation"] for g in geoms])
+        z = np.zeros((0, 64), np.int64)
+        return z, z, np.zeros(0, np.int64), np.zeros(len(ps), np.int8), 0.0, {}
+
+    monkeypatch.setattr(gpu, "coni_zpk_pfvs", fake_pfvs)
+    monkeypatch.setattr(dilation, "coni_dilation_bound_ceils", fake_bounds)
+    monkeypatch.setattr(gpu, "coni_pfvs_multi", fake_zpm)
+    items = []
+    for g in gs:
+        kappa, Mb, ps, h, Q, M0min = _geo(g)
+        items.append(dict(kappa=kappa, Mbasis=Mb, ps=ps[:, 1:], Q=Q, M0min=M0min))
+    for g, (Ks, Ms, keys) in zip(gs, zpk.coni_zpk_multi(items, D0)):
+        h = Ks.shape[1]
+        got = np.hstack([keys[:, None], Ms, Ks]) if len(keys) else np.zeros((0, 1 + 2 * h), np.int64)
+        np.testing.assert_array_equal(got, Z[f"g{g}_d{D0}_pfvs"], err_msg=f"geometry {g}")
+    assert not searched
+    # max_N_pfvs = 3: geometry 13's directions with more points go to ZpM at max(bound, D0) = 400
+    Ks, Ms, keys, info = zpk.coni_zpk(items[1]["kappa"], items[1]["Mbasis"], items[1]["ps"], items[1]["Q"], D0,
+                                      M0min=items[1]["M0min"], max_N_pfvs=3, return_info=True)
+    per = np.bincount(Z["g13_d20_points"][:, 0], minlength=len(items[1]["ps"]))
+    np.testing.assert_array_equal(info["fallback"], np.flatnonzero(per > 3))
+    assert searched == [[400.0]]
+    with pytest.raises(ValueError):
+        zpk.coni_zpk(items[1]["kappa"], items[1]["Mbasis"], items[1]["ps"], items[1]["Q"], 0)
