@@ -107,7 +107,7 @@ struct ZpkArgs {
     int h;
     const int64_t *kappa;                     // h^3
     const int64_t *Mbasis;                    // h^2
-    const int64_t *ps;                        // rows of ps_stride entries, p[0] = 0 in the first h
+    const int64_t *ps;                        // (n_p, ps_stride >= h), p[0] = 0 in the first h
     int ps_stride;
     int n_p;
     int64_t Q, M0min, D0, max_out;
@@ -117,7 +117,7 @@ struct ZpkArgs {
     unsigned long long *count;                // points emitted (all directions; may exceed cap)
     unsigned long long cap;                   // rows the output arrays hold
     int64_t *M, *Kn, *q, *pidx;               // rows of MH (first h entries), (cap,)
-    long long budget;                         // search nodes + (j, M0) steps per direction
+    long long budget;                         // search nodes + (j, M0) steps per lane and direction
 };
 
 // int128 quotient (truncated, as C) and remainder, on the 64-bit path when both
