@@ -12,7 +12,11 @@ vectors (tests/golden/zpk.npz, made by tests/golden/make_zpk_golden.py):
   reference), h11 beyond the kernel (-20), and directions without a bound
   (s > 0 or S not positive definite) status 1, as the reference's C code;
 - max_out: a direction with more points than max_out ends with -80 and
-  keeps none (the reference's rule).
+  keeps none (the reference's rule);
+- D0 = 1, 2, 5 (the most points per direction) on the h11 3..5 geometries
+  against the reference's czk_batch run here (where oracle/_ref is built);
+- the driver's host logic (pfvs_b200.zpk) with the emulated kernel and the
+  oracle's post-processing standing in for the device.
 """
 import os
 
@@ -152,3 +156,26 @@ def test_zpk_driver_host_logic(monkeypatch):
     assert searched == [[400.0]]
     with pytest.raises(ValueError):
         zpk.coni_zpk(items[1]["kappa"], items[1]["Mbasis"], items[1]["ps"], items[1]["Q"], 0)
+
+
+@pytest.mark.parametrize("D0", [1, 2, 5])
+def test_device_zpk_small_D0_against_the_reference_build(D0):
+    """Small D0 (the most points per direction) on the h11 3..5 dataset
+    geometries, 6 directions each: the emulated kernel against the
+    reference's own czk_batch (oracle/_ref) run here."""
+    from oracle import ref
+    if not ref.available():
+        pytest.skip("the reference's C build (oracle/_ref) is not present")
+    total = 0
+    for g in range(16):
+        kappa, Mb, ps, h, Q, M0min = _geo(g)
+        ps = ps[:6]
+        want = _rows(*ref.coni_zpk_batch(kappa, Mb, ps, Q, M0min, D0))
+        st_ref = ref.coni_zpk_batch(kappa, Mb, ps, Q, M0min, D0)[4]
+        M, Kn, q, pidx, st = emu.coni_zpk_batch(kappa, Mb, ps, Q, M0min, D0)
+        np.testing.assert_array_equal(st, st_ref, err_msg=f"geometry {g}")
+        got = _rows(M, Kn, q, pidx, st)
+        assert got.shape == want.shape, (g, D0)
+        np.testing.assert_array_equal(got, want, err_msg=f"geometry {g}")
+        total += len(want)
+    assert total > 500
